@@ -1,0 +1,74 @@
+// capi.cu - the C ABI's common entry points: version, errors (a thread-local message; a device error word that
+// kernels set instead of trapping), device information.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+
+static thread_local std::string g_err;
+
+void m25_set_error(const std::string &msg) { g_err = msg; }
+
+int m25_cuda_status(cudaError_t e, const char *where)
+{
+    g_err = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return M25_ECUDA;
+}
+
+// one device error word per device, allocated on first use
+static int *g_dev_err[64];
+static std::mutex g_mu;
+
+int *m25_dev_err_word()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_dev_err[dev]) {
+        int *p = nullptr;
+        if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+        cudaMemset(p, 0, sizeof(int));
+        cudaDeviceSynchronize();
+        g_dev_err[dev] = p;
+    }
+    return g_dev_err[dev];
+}
+
+extern "C" const char *m25_version(void) { return "mom25d_b200 0.1 (sm_100a)"; }
+
+extern "C" const char *m25_last_error(void) { return g_err.c_str(); }
+
+extern "C" int m25_device_info(int *sm_count, size_t *free_bytes, size_t *total_bytes)
+{
+    int dev = 0;
+    M25_CHECK(cudaGetDevice(&dev));
+    if (sm_count) M25_CHECK(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+    size_t f = 0, t = 0;
+    M25_CHECK(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return M25_OK;
+}
+
+// Synchronises the stream and reads (then clears) the device error word: M25_EDEVICE with the code if a kernel
+// reported one (an index out of range, a bounded wait that gave up, a zero pivot).
+extern "C" int m25_sync_check(void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    M25_CHECK(cudaStreamSynchronize(s));
+    int *w = m25_dev_err_word();
+    if (!w) { g_err = "m25_sync_check: no device error word"; return M25_ECUDA; }
+    int code = 0;
+    M25_CHECK(cudaMemcpy(&code, w, sizeof(int), cudaMemcpyDeviceToHost));
+    if (code) {
+        M25_CHECK(cudaMemset(w, 0, sizeof(int)));
+        char buf[128];
+        snprintf(buf, sizeof buf, "a kernel reported device code %d (%s)", code,
+                 code == M25_DEV_TIMEOUT ? "a bounded wait gave up" : code == M25_DEV_INDEX ? "index out of range" :
+                 code == M25_DEV_ZEROPIV ? "zero pivot: singular factor" : "unknown");
+        g_err = buf;
+        return M25_EDEVICE;
+    }
+    return M25_OK;
+}

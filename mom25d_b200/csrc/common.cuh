@@ -1,0 +1,130 @@
+// common.cuh - shared device helpers of libmom25d_b200: complex arithmetic on interleaved (re, im) pairs, the
+// packed mesh / table views the kernels read, a bounded grid barrier, and the error plumbing of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/mom25d_b200.h"
+
+// ---- complex arithmetic (interleaved re, im: the layout of numpy complex128 / complex64) ----------------------------
+template <typename R> struct cpx { R x, y; };
+template <typename R> struct vec2_of;
+template <> struct vec2_of<double> { typedef double2 type; };
+template <> struct vec2_of<float> { typedef float2 type; };
+
+template <typename R> __host__ __device__ __forceinline__ cpx<R> mk(R a, R b) { cpx<R> c; c.x = a; c.y = b; return c; }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator+(cpx<R> a, cpx<R> b) { return mk(a.x + b.x, a.y + b.y); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator-(cpx<R> a, cpx<R> b) { return mk(a.x - b.x, a.y - b.y); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator*(cpx<R> a, cpx<R> b) { return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator*(cpx<R> a, R s) { return mk(a.x * s, a.y * s); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator*(R s, cpx<R> a) { return mk(a.x * s, a.y * s); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> operator/(cpx<R> a, R s) { return mk(a.x / s, a.y / s); }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> &operator+=(cpx<R> &a, cpx<R> b) { a.x += b.x; a.y += b.y; return a; }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> &operator-=(cpx<R> &a, cpx<R> b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename R> __host__ __device__ __forceinline__ cpx<R> conj(cpx<R> a) { return mk(a.x, -a.y); }
+template <typename R> __host__ __device__ __forceinline__ R abs1(cpx<R> a) { return fabs(a.x) + fabs(a.y); }
+// a / b by Smith's method (the scaled quotient; no overflow for large |b|)
+template <typename R> __host__ __device__ __forceinline__ cpx<R> cdiv(cpx<R> a, cpx<R> b)
+{
+    if (fabs(b.x) >= fabs(b.y)) {
+        R r = b.y / b.x, d = b.x + b.y * r;
+        return mk((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+    }
+    R r = b.x / b.y, d = b.x * r + b.y;
+    return mk((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+// a += b * c
+template <typename R> __host__ __device__ __forceinline__ void cfma(cpx<R> &a, cpx<R> b, cpx<R> c)
+{
+    a.x = fma(b.x, c.x, a.x); a.x = fma(-b.y, c.y, a.x);
+    a.y = fma(b.x, c.y, a.y); a.y = fma(b.y, c.x, a.y);
+}
+// a -= b * c
+template <typename R> __host__ __device__ __forceinline__ void cfms(cpx<R> &a, cpx<R> b, cpx<R> c)
+{
+    a.x = fma(-b.x, c.x, a.x); a.x = fma(b.y, c.y, a.x);
+    a.y = fma(-b.x, c.y, a.y); a.y = fma(-b.y, c.x, a.y);
+}
+
+typedef cpx<double> zd;
+typedef cpx<float> zf;
+
+template <typename R> __device__ __forceinline__ cpx<R> ldc(const R *p, size_t i)
+{
+    typedef typename vec2_of<R>::type V;
+    V v = reinterpret_cast<const V *>(p)[i];
+    return mk(v.x, v.y);
+}
+template <typename R> __device__ __forceinline__ void stc(R *p, size_t i, cpx<R> c)
+{
+    typedef typename vec2_of<R>::type V;
+    V v; v.x = c.x; v.y = c.y;
+    reinterpret_cast<V *>(p)[i] = v;
+}
+
+// ---- error plumbing ---------------------------------------------------------------------------------------------------
+void m25_set_error(const std::string &msg);
+int m25_cuda_status(cudaError_t e, const char *where);
+#define M25_CHECK(call)                                                                                    \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return m25_cuda_status(e_, #call);                                          \
+    } while (0)
+#define M25_LAUNCH_CHECK(what)                                                                             \
+    do {                                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                                               \
+        if (e_ != cudaSuccess) return m25_cuda_status(e_, what);                                           \
+    } while (0)
+#define M25_REQUIRE(cond, msg)                                                                             \
+    do {                                                                                                   \
+        if (!(cond)) { m25_set_error(msg); return M25_EINVAL; }                                            \
+    } while (0)
+
+// device-side error word: kernels that detect a bad index or a barrier that gave up write a code here (never trap)
+__device__ __forceinline__ void dev_error(int *err, int code)
+{
+    if (err) atomicCAS(err, 0, code);
+}
+
+// ---- a bounded grid barrier for cooperative (co-resident) launches -------------------------------------------------
+// count / gen live in global memory (zeroed before the launch). Every block arrives once per phase; the last one
+// bumps the generation. A wait that exceeds `limit` polls records M25_DEV_TIMEOUT in *err and returns false, so a
+// stuck phase ends the kernel instead of hanging the GPU.
+struct GridBarrier {
+    unsigned *count;
+    unsigned *gen;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned nblocks, unsigned &phase, int *err)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        unsigned target = phase + 1;
+        if (atomicAdd(b.count, 1u) == nblocks * target - 1) {
+            __threadfence();
+            atomicExch(b.gen, target);
+        } else {
+            long it = 0;
+            while (ld_acquire_u32(b.gen) < target) {
+                if (++it > (1L << 26)) { ok = 0; dev_error(err, M25_DEV_TIMEOUT); break; }
+                if (err && *(volatile int *)err) { ok = 0; break; }
+                __nanosleep(20);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    phase += 1;
+    return ok;
+}

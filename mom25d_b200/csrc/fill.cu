@@ -1,0 +1,657 @@
+// fill.cu - the per-frequency impedance-matrix fill on the GPU: centroid-rule far field, near-field correction,
+// near-pair search, via-fan charge moments, radial-table sums, the matrix-free far-field product and the symmetric
+// equilibration. Restates mom25d_core.cpp (cited per kernel) with one thread per matrix entry / triangle pair.
+#include "common.cuh"
+
+// ---- the tabulated kernel (mom25d_core.cpp:64-90) ---------------------------------------------------------------------
+// TB: m25_tables (complex128 samples) or m25_tables_f (complex64); R the arithmetic precision.
+template <typename R, typename TB>
+__device__ __forceinline__ void tab_rest(const TB &tb, int t, R r, cpx<R> &ga, cpx<R> &gq)
+{
+    R u = r / (R)tb.dr[t];
+    const R umax = (R)tb.nfine - (R)1.000001;
+    if (u > umax) u = umax;
+    int i = (int)u;
+    R f = u - (R)i;
+    size_t o = (size_t)t * tb.nfine + i;
+    cpx<R> a0 = ldc<R>((const R *)tb.A, o), a1 = ldc<R>((const R *)tb.A, o + 1);
+    cpx<R> q0 = ldc<R>((const R *)tb.Q, o), q1 = ldc<R>((const R *)tb.Q, o + 1);
+    ga = a0 * (1 - f) + a1 * f;
+    gq = q0 * (1 - f) + q1 * f;
+}
+
+template <typename R, typename TB>
+__device__ __forceinline__ void tab_kern(const TB &tb, int la, int lb, R r, cpx<R> &ga, cpx<R> &gq)
+{
+    int t = tb.tab[la * tb.L + lb];
+    tab_rest<R>(tb, t, r, ga, gq);
+    int kd = tb.kind[t];
+    if (kd == 0) {
+        if (r > 0) {
+            ga += ldc<R>((const R *)tb.cA, t) / r;
+            gq += ldc<R>((const R *)tb.cq, t) / r;
+        }
+        R di = (R)tb.dimg[t];
+        if (di > 0) {
+            R ri = (R)1 / sqrt(r * r + di * di);
+            ga += ldc<R>((const R *)tb.cAi, t) * ri;
+            gq += ldc<R>((const R *)tb.cqi, t) * ri;
+        }
+    } else if (kd == 1) {
+        R dd = (R)tb.d[t];
+        R ri = (R)1 / sqrt(r * r + dd * dd);
+        ga += ldc<R>((const R *)tb.cA, t) * ri;
+        gq += ldc<R>((const R *)tb.cq, t) * ri;
+    }
+}
+
+// centroid distance: the differences in double (nearby triangles' coordinates cancel), the root in R
+template <typename R>
+__device__ __forceinline__ R cdist(const double *c, int p, int q)
+{
+    double dx = c[2 * p] - c[2 * q], dy = c[2 * p + 1] - c[2 * q + 1];
+    return sqrt((R)(dx * dx + dy * dy));
+}
+
+// ---- far field: fill_far (mom25d_core.cpp:132-173) ----------------------------------------------------------------
+// One thread per entry (m, n), evaluated in the reference's order for the pair (min(m, n), max(m, n)) so that Z is
+// exactly symmetric, as the reference writes it. A 32 x 32 tile per block; the tile's 64 edges staged in shared
+// memory (their triangles, alpha x area and centroid - free vertex vectors).
+struct EdgeHalves { int p[2]; int lt[2]; double a[2], dx[2], dy[2]; };
+
+template <typename R, typename TB>
+__global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB tb, double w)
+{
+    __shared__ EdgeHalves rows[32], cols[32];
+    const int M0 = blockIdx.y * 32, N0 = blockIdx.x * 32;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid < 64) {
+        int e = (tid < 32 ? M0 : N0) + (tid & 31);
+        EdgeHalves h;
+        if (e < g.Ne) {
+            int pp = g.ep[e], pm = g.em[e];
+            h.p[0] = pp; h.p[1] = pm;
+            h.lt[0] = g.lt[pp]; h.lt[1] = g.lt[pm];
+            h.a[0] = g.ap[e] * g.area[pp]; h.a[1] = g.am[e] * g.area[pm];
+            h.dx[0] = g.cent[2 * pp] - g.vp[2 * e]; h.dy[0] = g.cent[2 * pp + 1] - g.vp[2 * e + 1];
+            h.dx[1] = g.cent[2 * pm] - g.vm[2 * e]; h.dy[1] = g.cent[2 * pm + 1] - g.vm[2 * e + 1];
+        } else {
+            h.p[0] = h.p[1] = 0; h.lt[0] = h.lt[1] = 0; h.a[0] = h.a[1] = 0; h.dx[0] = h.dx[1] = h.dy[0] = h.dy[1] = 0;
+        }
+        (tid < 32 ? rows : cols)[tid & 31] = h;
+    }
+    __syncthreads();
+    const int n = N0 + threadIdx.x;
+    if (n >= g.Ne) return;
+    const cpx<R> jw = mk<R>(0, (R)w);
+    const cpx<R> inv_jw = mk<R>(0, (R)(-1.0 / w));
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const int m = M0 + i;
+        if (m >= g.Ne) break;
+        const EdgeHalves &A = (m <= n) ? rows[i] : cols[threadIdx.x];
+        const EdgeHalves &B = (m <= n) ? cols[threadIdx.x] : rows[i];
+        cpx<R> v = mk<R>(0, 0);
+        for (int s = 0; s < 2; ++s)
+            for (int t = 0; t < 2; ++t) {
+                cpx<R> ga, gq;
+                tab_kern<R>(tb, A.lt[s], B.lt[t], cdist<R>(g.cent, A.p[s], B.p[t]), ga, gq);
+                R dot = (R)A.dx[s] * (R)B.dx[t] + (R)A.dy[s] * (R)B.dy[t];
+                cpx<R> term = (jw * dot) * ga + (gq * (R)4) * inv_jw;
+                v += ((R)A.a[s] * (R)B.a[t]) * term;
+            }
+        stc<R>(Z, (size_t)m * ld + n, v);
+    }
+}
+
+// far_block (mom25d_core.cpp:176-211): arbitrary row / column edge lists, complex128 out
+template <typename TB>
+__global__ void k_far_block(const int *R_, int nr, const int *C_, int nc, double *out, m25_mesh g, TB tb, double w)
+{
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)nr * nc) return;
+    int i = idx / nc, j = idx % nc;
+    int m = R_[i], n = C_[j];
+    const zd jw = mk<double>(0, w), inv_jw = mk<double>(0, -1.0 / w);
+    int pm[2] = {g.ep[m], g.em[m]}, pn[2] = {g.ep[n], g.em[n]};
+    double am_[2] = {g.ap[m] * g.area[pm[0]], g.am[m] * g.area[pm[1]]};
+    double dx[2] = {g.cent[2 * pm[0]] - g.vp[2 * m], g.cent[2 * pm[1]] - g.vm[2 * m]};
+    double dy[2] = {g.cent[2 * pm[0] + 1] - g.vp[2 * m + 1], g.cent[2 * pm[1] + 1] - g.vm[2 * m + 1]};
+    double an[2] = {g.ap[n] * g.area[pn[0]], g.am[n] * g.area[pn[1]]};
+    double ex[2] = {g.cent[2 * pn[0]] - g.vp[2 * n], g.cent[2 * pn[1]] - g.vm[2 * n]};
+    double ey[2] = {g.cent[2 * pn[0] + 1] - g.vp[2 * n + 1], g.cent[2 * pn[1] + 1] - g.vm[2 * n + 1]};
+    zd v = mk<double>(0, 0);
+    for (int s = 0; s < 2; ++s)
+        for (int t = 0; t < 2; ++t) {
+            zd ga, gq;
+            tab_kern<double>(tb, g.lt[pm[s]], g.lt[pn[t]], cdist<double>(g.cent, pm[s], pn[t]), ga, gq);
+            zd term = (jw * (dx[s] * ex[t] + dy[s] * ey[t])) * ga + (gq * 4.0) * inv_jw;
+            v += (am_[s] * an[t]) * term;
+        }
+    stc<double>(out, idx, v);
+}
+
+// ---- analytic 1/sqrt(rho^2 + d^2) moments (mom25d_core.cpp:321-365) ---------------------------------------------------
+__device__ __forceinline__ bool rule_over_p(double ap, double aq, int p, int q)
+{
+    const double tie = 1e-9 * fmax(ap, aq);
+    return fabs(ap - aq) <= tie ? p <= q : ap < aq;
+}
+
+__device__ void offplane_one(const double *V, const double *P6, const double *W6, double d, double m[6], bool keep)
+{
+    double ad = fabs(d);
+    double e[3][2], L[3], tau[3][2], un[3][2];
+    for (int i = 0; i < 3; ++i) {
+        int j = (i + 1) % 3;
+        e[i][0] = V[2 * j] - V[2 * i]; e[i][1] = V[2 * j + 1] - V[2 * i + 1];
+        L[i] = sqrt(e[i][0] * e[i][0] + e[i][1] * e[i][1]);
+        tau[i][0] = e[i][0] / L[i]; tau[i][1] = e[i][1] / L[i];
+        un[i][0] = tau[i][1]; un[i][1] = -tau[i][0];
+    }
+    double m0 = 0, mro0 = 0, mro1 = 0, mrs0 = 0, mrs1 = 0, mrr = 0;
+    for (int k = 0; k < 6; ++k) {
+        double rx = P6[2 * k], ry = P6[2 * k + 1], wq = W6[k];
+        double I1 = 0, IRx = 0, IRy = 0;
+        for (int i = 0; i < 3; ++i) {
+            double dvx = V[2 * i] - rx, dvy = V[2 * i + 1] - ry;
+            double sm = dvx * tau[i][0] + dvy * tau[i][1];
+            double sp = sm + L[i];
+            double t0 = dvx * un[i][0] + dvy * un[i][1];
+            double R02 = t0 * t0 + d * d, R0 = sqrt(R02);
+            double Rm = sqrt(R02 + sm * sm), Rp = sqrt(R02 + sp * sp);
+            double lg = (R0 > 1e-14 * L[i]) ? asinh(sp / R0) - asinh(sm / R0) : 0.0;
+            double beta = atan2(t0 * sp, R02 + ad * Rp) - atan2(t0 * sm, R02 + ad * Rm);
+            I1 += t0 * lg - ad * beta;
+            double eR = 0.5 * (R02 * lg + sp * Rp - sm * Rm);
+            IRx += eR * un[i][0]; IRy += eR * un[i][1];
+        }
+        double Wx = IRx + rx * I1, Wy = IRy + ry * I1;
+        m0 += wq * I1;
+        mro0 += wq * rx * I1; mro1 += wq * ry * I1;
+        mrs0 += wq * Wx; mrs1 += wq * Wy;
+        mrr += wq * (rx * Wx + ry * Wy);
+    }
+    // observation- / source-weighted moments handed back as (p, q) whichever triangle carried the rule
+    m[0] = m0;
+    if (keep) { m[1] = mro0; m[2] = mro1; m[3] = mrs0; m[4] = mrs1; }
+    else { m[1] = mrs0; m[2] = mrs1; m[3] = mro0; m[4] = mro1; }
+    m[5] = mrr;
+}
+
+// ---- near-field correction (near_core, mom25d_core.cpp:417-507) -----------------------------------------------------
+// One thread per near pair. mode 0: atomically added into Z (R_out = double or float); mode 2: COO triplets.
+template <typename Zt>
+__device__ __forceinline__ void atomic_add_c(Zt *Z, size_t i, zd v);
+template <> __device__ __forceinline__ void atomic_add_c<double>(double *Z, size_t i, zd v)
+{
+    atomicAdd(Z + 2 * i, v.x); atomicAdd(Z + 2 * i + 1, v.y);
+}
+template <> __device__ __forceinline__ void atomic_add_c<float>(float *Z, size_t i, zd v)
+{
+    atomicAdd(Z + 2 * i, (float)v.x); atomicAdd(Z + 2 * i + 1, (float)v.y);
+}
+
+template <typename Zt>
+__global__ void __launch_bounds__(128) k_near(int mode, Zt *Z, long ld, int *ri, int *ci, double *vv, double *qcorr,
+                                              double *stat, int stat_ready, m25_mesh g, m25_tables tb, m25_quad q,
+                                              const int *P, const int *Q, long n, double w, int *err)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const zd jw = mk<double>(0, w), inv_jw = mk<double>(0, -1.0 / w);
+    const int p = P[i], qq = Q[i];
+    if (p < 0 || p >= g.Nt || qq < 0 || qq >= g.Nt) { dev_error(err, M25_DEV_INDEX); return; }
+    const int la = g.lt[p], lb = g.lt[qq];
+    const int t = tb.tab[la * tb.L + lb];
+    const bool same = (la == lb);
+    const int np = same ? 3 : 6;
+    const double *Pa = same ? q.P3 + 6 * (size_t)p : q.P6 + 12 * (size_t)p;
+    const double *Pb = same ? q.P3 + 6 * (size_t)qq : q.P6 + 12 * (size_t)qq;
+    const double *Wa = same ? q.W3 + 3 * (size_t)p : q.W6 + 6 * (size_t)p;
+    const double *Wb = same ? q.W3 + 3 * (size_t)qq : q.W6 + 6 * (size_t)qq;
+    zd M0 = mk<double>(0, 0), Mox = M0, Moy = M0, Msx = M0, Msy = M0, Mrr = M0, Mq = M0;
+    double pbx[6], pby[6], wb[6];
+    for (int b = 0; b < np; ++b) { pbx[b] = Pb[2 * b]; pby[b] = Pb[2 * b + 1]; wb[b] = Wb[b]; }
+    for (int a = 0; a < np; ++a) {
+        const double pax = Pa[2 * a], pay = Pa[2 * a + 1], wa = Wa[a];
+        for (int b = 0; b < np; ++b) {
+            double dx = pax - pbx[b], dy = pay - pby[b];
+            zd ga, gq;
+            tab_rest<double>(tb, t, sqrt(dx * dx + dy * dy), ga, gq);
+            double wt = wa * wb[b];
+            ga = ga * wt; gq = gq * wt;
+            M0 += ga; Mox += ga * pax; Moy += ga * pay;
+            Msx += ga * pbx[b]; Msy += ga * pby[b];
+            Mrr += ga * (pax * pbx[b] + pay * pby[b]);
+            Mq += gq;
+        }
+    }
+    const bool keep = rule_over_p(g.area[p], g.area[qq], p, qq);
+    const int po = keep ? p : qq, qi = keep ? qq : p;
+    double V[6];
+    for (int k = 0; k < 3; ++k) {
+        int nd = q.tris[3 * qi + k];
+        V[2 * k] = q.nodes[2 * nd]; V[2 * k + 1] = q.nodes[2 * nd + 1];
+    }
+    const int kd = tb.kind[t];
+    const int nk = kd == 0 ? (tb.dimg[t] > 0 ? 2 : 1) : (kd == 1 ? 1 : 0);
+    for (int k = 0; k < nk; ++k) {
+        double dd = kd == 0 ? (k == 0 ? 0.0 : tb.dimg[t]) : tb.d[t];
+        zd cA = (k == 0) ? ldc<double>(tb.cA, t) : ldc<double>(tb.cAi, t);
+        zd cq = (k == 0) ? ldc<double>(tb.cq, t) : ldc<double>(tb.cqi, t);
+        double m[6];
+        double *st = stat ? stat + 12 * (size_t)i + 6 * k : nullptr;
+        if (st && stat_ready) {
+            for (int j = 0; j < 6; ++j) m[j] = st[j];
+        } else {
+            offplane_one(V, q.P6 + 12 * (size_t)po, q.W6 + 6 * (size_t)po, dd, m, keep);
+            if (st) for (int j = 0; j < 6; ++j) st[j] = m[j];
+        }
+        M0 += cA * m[0]; Mox += cA * m[1]; Moy += cA * m[2]; Msx += cA * m[3]; Msy += cA * m[4];
+        Mrr += cA * m[5]; Mq += cq * m[0];
+    }
+    {
+        double r = cdist<double>(g.cent, p, qq);
+        zd ga, gq;
+        tab_kern<double>(tb, la, lb, r, ga, gq);
+        double wgt = g.area[p] * g.area[qq];
+        double cpx_ = g.cent[2 * p], cpy = g.cent[2 * p + 1], cqx = g.cent[2 * qq], cqy = g.cent[2 * qq + 1];
+        ga = ga * wgt; gq = gq * wgt;
+        M0 -= ga; Mox -= ga * cpx_; Moy -= ga * cpy; Msx -= ga * cqx; Msy -= ga * cqy;
+        Mrr -= ga * (cpx_ * cqx + cpy * cqy); Mq -= gq;
+    }
+    if (qcorr) stc<double>(qcorr, i, Mq);
+    for (int s = 0; s < 3; ++s) {
+        int em_ = g.te[3 * p + s];
+        for (int u = 0; u < 3; ++u) {
+            int en = g.te[3 * qq + u];
+            size_t slot = 9 * (size_t)i + 3 * s + u;
+            if (em_ < 0 || en < 0) {
+                if (mode == 2) { ri[slot] = -1; ci[slot] = 0; vv[2 * slot] = 0; vv[2 * slot + 1] = 0; }
+                continue;
+            }
+            double am_ = g.ta[3 * p + s], vx = g.tv[6 * p + 2 * s], vy = g.tv[6 * p + 2 * s + 1];
+            double an = g.ta[3 * qq + u], wx = g.tv[6 * qq + 2 * u], wy = g.tv[6 * qq + 2 * u + 1];
+            zd Acomb = Mrr - (Mox * wx + Moy * wy) - (Msx * vx + Msy * vy) + M0 * (vx * wx + vy * wy);
+            zd val = (am_ * an) * (jw * Acomb + (Mq * 4.0) * inv_jw);
+            if (mode == 0) atomic_add_c<Zt>(Z, (size_t)em_ * ld + en, val);
+            else { ri[slot] = em_; ci[slot] = en; stc<double>(vv, slot, val); }
+        }
+    }
+}
+
+// ---- near pairs (mom25d_core.cpp:1216-1263): brute force over all pairs, rows in order -------------------------------
+__global__ void k_near_count(const double *c, const double *sz, const double *zz, int Nt, double fac, long long *cnt)
+{
+    // one warp per row p
+    int p = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (p >= Nt) return;
+    double cx = c[2 * p], cy = c[2 * p + 1], zp = zz[p], sp = sz[p];
+    long long k = 0;
+    for (int q = lane; q < Nt; q += 32) {
+        double dx = cx - c[2 * q], dy = cy - c[2 * q + 1], dz = zp - zz[q];
+        double R = fac * fmax(sp, sz[q]);
+        k += (dx * dx + dy * dy + dz * dz < R * R);
+    }
+    for (int o = 16; o; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if (lane == 0) cnt[p] = k;
+}
+
+__global__ void k_near_fill(const double *c, const double *sz, const double *zz, int Nt, double fac,
+                            const long long *off, int *P, int *Q)
+{
+    int p = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (p >= Nt) return;
+    double cx = c[2 * p], cy = c[2 * p + 1], zp = zz[p], sp = sz[p];
+    long long base = off[p];
+    for (int q0 = 0; q0 < Nt; q0 += 32) {
+        int q = q0 + lane;
+        bool hit = false;
+        if (q < Nt) {
+            double dx = cx - c[2 * q], dy = cy - c[2 * q + 1], dz = zp - zz[q];
+            double R = fac * fmax(sp, sz[q]);
+            hit = dx * dx + dy * dy + dz * dz < R * R;
+        }
+        unsigned msk = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            long long k = base + __popc(msk & ((1u << lane) - 1));
+            P[k] = p; Q[k] = q;
+        }
+        base += __popc(msk);
+    }
+}
+
+__global__ void k_exclusive_scan_small(long long *a, int n, long long *total)
+{
+    // single block, serial chunks: n is the triangle count (<= a few 1e5)
+    __shared__ long long part[1024];
+    int t = threadIdx.x, nt = blockDim.x;
+    int chunk = (n + nt - 1) / nt, b = t * chunk, e = min(n, b + chunk);
+    long long s = 0;
+    for (int i = b; i < e; ++i) s += a[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        long long acc = 0;
+        for (int i = 0; i < nt; ++i) { long long v = part[i]; part[i] = acc; acc += v; }
+        *total = acc;
+    }
+    __syncthreads();
+    long long acc = part[t];
+    for (int i = b; i < e; ++i) { long long v = a[i]; a[i] = acc; acc += v; }
+    if (t == nt - 1) a[n] = *total;
+}
+
+// ---- fan charges (fan_q, mom25d_core.cpp:1585-1603) -----------------------------------------------------------------
+__global__ void k_fan_q(const int *F, int nf, double *out, m25_mesh g, m25_tables tb)
+{
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)g.Nt * nf) return;
+    int t = idx / nf, j = idx % nf, f = F[j];
+    zd ga, gq;
+    tab_kern<double>(tb, g.lt[t], g.lt[f], cdist<double>(g.cent, t, f), ga, gq);
+    stc<double>(out, idx, gq * (g.area[t] * g.area[f]));
+}
+
+// ---- radial table sums (radial_table_sum, mom25d_core.cpp:1269-1298) ------------------------------------------------
+__global__ void k_radial_table_sum(const double *x, const double *y, const double *W, long nt, int nq,
+                                   const double *ax, const double *ay, int nv, const double *D, long n, double dr,
+                                   double *out)
+{
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= nt * nv) return;
+    long t = idx / nv;
+    int v = idx % nv;
+    const double top = (double)n - 1.000001;
+    zd acc = mk<double>(0, 0);
+    for (int q = 0; q < nq; ++q) {
+        const double rx = x[t * nq + q] - ax[v], ry = y[t * nq + q] - ay[v];
+        double u = fmin(hypot(rx, ry) / dr, top);
+        long i = (long)u;
+        double f = u - (double)i;
+        acc += (ldc<double>(D, i) * (1.0 - f) + ldc<double>(D, i + 1) * f) * W[t * nq + q];
+    }
+    stc<double>(out, idx, acc);
+}
+
+// ---- matrix-free far product (matvec_far_multi, mom25d_core.cpp:257-314) --------------------------------------------
+// 1. per triangle: s0 = sum a A x, s1 = sum a A x (c - v) over the halves on it (gathered through te / ta / tv)
+__global__ void k_mv_aggregate(const double *X, int K, m25_mesh g, double *s0, double *s1x, double *s1y)
+{
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)g.Nt * K) return;
+    int t = idx / K, c = idx % K;
+    zd a0 = mk<double>(0, 0), ax = a0, ay = a0;
+    for (int s = 0; s < 3; ++s) {
+        int e = g.te[3 * t + s];
+        if (e < 0) continue;
+        zd x = ldc<double>(X, (size_t)e * K + c);
+        zd a = x * (g.ta[3 * t + s] * g.area[t]);
+        a0 += a;
+        ax += a * (g.cent[2 * t] - g.tv[6 * t + 2 * s]);
+        ay += a * (g.cent[2 * t + 1] - g.tv[6 * t + 2 * s + 1]);
+    }
+    stc<double>(s0, idx, a0); stc<double>(s1x, idx, ax); stc<double>(s1y, idx, ay);
+}
+
+// 2. vAx[p] = sum_q GA(p, q) s1x[q], vAy likewise, wQ[p] = sum_q GQ(p, q) s0[q]: a block of 128 observation
+//    triangles per CTA, source triangles streamed through shared memory; K <= 16 columns.
+template <int KMAX>
+__global__ void __launch_bounds__(128) k_mv_pairs(int K, m25_mesh g, m25_tables tb, const double *s0,
+                                                  const double *s1x, const double *s1y, double *vAx, double *vAy,
+                                                  double *wQ)
+{
+    constexpr int QT = KMAX <= 8 ? 64 : 32;            // source triangles a stage (48 KB of static shared memory)
+    __shared__ double sc[QT][2];
+    __shared__ int sl[QT];
+    __shared__ zd S0[QT][KMAX], SX[QT][KMAX], SY[QT][KMAX];
+    const int p = blockIdx.x * 128 + threadIdx.x;
+    const bool live = p < g.Nt;
+    const double cx = live ? g.cent[2 * p] : 0, cy = live ? g.cent[2 * p + 1] : 0;
+    const int lp = live ? g.lt[p] : 0;
+    zd ax[KMAX], ay[KMAX], aq[KMAX];
+    for (int c = 0; c < KMAX; ++c) ax[c] = ay[c] = aq[c] = mk<double>(0, 0);
+    for (int q0 = 0; q0 < g.Nt; q0 += QT) {
+        __syncthreads();
+        for (int j = threadIdx.x; j < QT; j += 128) {
+            int q = q0 + j;
+            sc[j][0] = q < g.Nt ? g.cent[2 * q] : 0; sc[j][1] = q < g.Nt ? g.cent[2 * q + 1] : 0;
+            sl[j] = q < g.Nt ? g.lt[q] : 0;
+        }
+        for (int j = threadIdx.x; j < QT * K; j += 128) {
+            int qq = j / K, c = j % K, q = q0 + qq;
+            zd z0 = mk<double>(0, 0);
+            S0[qq][c] = q < g.Nt ? ldc<double>(s0, (size_t)q * K + c) : z0;
+            SX[qq][c] = q < g.Nt ? ldc<double>(s1x, (size_t)q * K + c) : z0;
+            SY[qq][c] = q < g.Nt ? ldc<double>(s1y, (size_t)q * K + c) : z0;
+        }
+        __syncthreads();
+        if (!live) continue;
+        int qn = min(QT, g.Nt - q0);
+        for (int j = 0; j < qn; ++j) {
+            double dx = cx - sc[j][0], dy = cy - sc[j][1];
+            zd ga, gq;
+            tab_kern<double>(tb, lp, sl[j], sqrt(dx * dx + dy * dy), ga, gq);
+#pragma unroll
+            for (int c = 0; c < KMAX; ++c) {
+                if (c < K) { ax[c] += ga * SX[j][c]; ay[c] += ga * SY[j][c]; aq[c] += gq * S0[j][c]; }
+            }
+        }
+    }
+    if (!live) return;
+    for (int c = 0; c < K; ++c) {
+        stc<double>(vAx, (size_t)p * K + c, ax[c]); stc<double>(vAy, (size_t)p * K + c, ay[c]);
+        stc<double>(wQ, (size_t)p * K + c, aq[c]);
+    }
+}
+
+// 3. Y[e] from the two halves' triangle sums
+__global__ void k_mv_finish(int K, m25_mesh g, double w, const double *vAx, const double *vAy, const double *wQ,
+                            double *Y)
+{
+    long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)g.Ne * K) return;
+    int e = idx / K, c = idx % K;
+    const zd jw = mk<double>(0, w), inv_jw = mk<double>(0, -1.0 / w);
+    int p = g.ep[e], q = g.em[e];
+    double dpx = g.cent[2 * p] - g.vp[2 * e], dpy = g.cent[2 * p + 1] - g.vp[2 * e + 1];
+    double dqx = g.cent[2 * q] - g.vm[2 * e], dqy = g.cent[2 * q + 1] - g.vm[2 * e + 1];
+    size_t ip = (size_t)p * K + c, iq = (size_t)q * K + c;
+    zd yp = (jw * (ldc<double>(vAx, ip) * dpx + ldc<double>(vAy, ip) * dpy) + (ldc<double>(wQ, ip) * 4.0) * inv_jw)
+            * (g.ap[e] * g.area[p]);
+    zd ym = (jw * (ldc<double>(vAx, iq) * dqx + ldc<double>(vAy, iq) * dqy) + (ldc<double>(wQ, iq) * 4.0) * inv_jw)
+            * (g.am[e] * g.area[q]);
+    stc<double>(Y, idx, yp + ym);
+}
+
+// ---- equilibration (fast.py:294-305; scale_c64, mom25d_core.cpp:1563-1580) ------------------------------------------
+__global__ void k_diag_scale(const double *Z, long n, long ld, double *d)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    zd z = ldc<double>(Z, (size_t)i * ld + i);
+    d[i] = 1.0 / sqrt(hypot(z.x, z.y) + 1e-300);
+}
+
+__global__ void k_diag_scale_c64(const float *Z, long n, long ld, double *d)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    zf z = ldc<float>(Z, (size_t)i * ld + i);
+    d[i] = 1.0 / sqrt(hypot((double)z.x, (double)z.y) + 1e-300);
+}
+
+__global__ void k_equilibrate_c64(float *Z, long n, long ld, const double *d)
+{
+    long i = blockIdx.y;
+    double di = d[i];
+    for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
+        zf z = ldc<float>(Z, (size_t)i * ld + j);
+        float s = (float)(di * d[j]);
+        stc<float>(Z, (size_t)i * ld + j, mk<float>(z.x * s, z.y * s));
+    }
+}
+
+__global__ void k_equilibrate(double *Z, long n, long ld, const double *d, float *Z64)
+{
+    long i = blockIdx.y;
+    double di = d[i];
+    for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
+        zd z = ldc<double>(Z, (size_t)i * ld + j) * (di * d[j]);
+        stc<double>(Z, (size_t)i * ld + j, z);
+        if (Z64) stc<float>(Z64, (size_t)i * n + j, mk<float>((float)z.x, (float)z.y));
+    }
+}
+
+// ======================================================================================================================
+// C ABI
+// ======================================================================================================================
+static inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+int *m25_dev_err_word();
+int m25_check_dev_err(cudaStream_t s, const char *what);
+
+extern "C" int m25_fill_far(void *d_Z, long ld, int single, const m25_mesh *g, const m25_tables *tb,
+                            const m25_tables_f *tbf, double w, void *stream)
+{
+    M25_REQUIRE(d_Z && g && ld >= g->Ne, "m25_fill_far: Z, g and ld >= Ne required");
+    if (g->Ne == 0) return M25_OK;
+    dim3 grid((g->Ne + 31) / 32, (g->Ne + 31) / 32), block(32, 8);
+    if (single) {
+        M25_REQUIRE(tbf, "m25_fill_far: single precision needs the complex64 tables");
+        k_fill_far<float, m25_tables_f><<<grid, block, 0, S(stream)>>>((float *)d_Z, ld, *g, *tbf, w);
+    } else {
+        M25_REQUIRE(tb, "m25_fill_far: the complex128 tables are required");
+        k_fill_far<double, m25_tables><<<grid, block, 0, S(stream)>>>((double *)d_Z, ld, *g, *tb, w);
+    }
+    M25_LAUNCH_CHECK("k_fill_far");
+    return M25_OK;
+}
+
+extern "C" int m25_far_block(const int *d_rows, int nr, const int *d_cols, int nc, double *d_out, const m25_mesh *g,
+                             const m25_tables *tb, double w, void *stream)
+{
+    M25_REQUIRE(g && tb && d_out, "m25_far_block: null argument");
+    long tot = (long)nr * nc;
+    if (!tot) return M25_OK;
+    k_far_block<m25_tables><<<(tot + 255) / 256, 256, 0, S(stream)>>>(d_rows, nr, d_cols, nc, d_out, *g, *tb, w);
+    M25_LAUNCH_CHECK("k_far_block");
+    return M25_OK;
+}
+
+extern "C" int m25_near(int mode, void *d_Z, long ld, int single, int *d_ri, int *d_ci, double *d_vv, double *d_qcorr,
+                        double *d_stat, int stat_ready, const m25_mesh *g, const m25_tables *tb, const m25_quad *q,
+                        const int *d_P, const int *d_Q, long n, double w, void *stream)
+{
+    M25_REQUIRE(g && tb && q, "m25_near: null argument");
+    M25_REQUIRE(mode == 0 || mode == 2, "m25_near: mode 0 (dense) or 2 (COO)");
+    M25_REQUIRE(mode != 0 || (d_Z && ld >= g->Ne), "m25_near: mode 0 needs Z");
+    M25_REQUIRE(mode != 2 || (d_ri && d_ci && d_vv), "m25_near: mode 2 needs ri, ci, vv");
+    if (n == 0) return M25_OK;
+    int *err = m25_dev_err_word();
+    long blocks = (n + 127) / 128;
+    if (single)
+        k_near<float><<<blocks, 128, 0, S(stream)>>>(mode, (float *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
+                                                     stat_ready, *g, *tb, *q, d_P, d_Q, n, w, err);
+    else
+        k_near<double><<<blocks, 128, 0, S(stream)>>>(mode, (double *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
+                                                      stat_ready, *g, *tb, *q, d_P, d_Q, n, w, err);
+    M25_LAUNCH_CHECK("k_near");
+    return M25_OK;
+}
+
+extern "C" int m25_near_pairs(const double *d_cent, const double *d_size, const double *d_z, int Nt, double fac,
+                              long long *d_offsets, long long *h_total, int *d_P, int *d_Q, void *stream)
+{
+    M25_REQUIRE(d_cent && d_size && d_z && d_offsets && h_total, "m25_near_pairs: null argument");
+    int blocks = (Nt + 7) / 8;
+    if (!d_P) {
+        long long *d_tot = d_offsets + Nt;
+        k_near_count<<<blocks, 256, 0, S(stream)>>>(d_cent, d_size, d_z, Nt, fac, d_offsets);
+        M25_LAUNCH_CHECK("k_near_count");
+        k_exclusive_scan_small<<<1, 1024, 0, S(stream)>>>(d_offsets, Nt, d_tot);
+        M25_LAUNCH_CHECK("k_exclusive_scan_small");
+        M25_CHECK(cudaMemcpyAsync(h_total, d_tot, sizeof(long long), cudaMemcpyDeviceToHost, S(stream)));
+        M25_CHECK(cudaStreamSynchronize(S(stream)));
+        return M25_OK;
+    }
+    k_near_fill<<<blocks, 256, 0, S(stream)>>>(d_cent, d_size, d_z, Nt, fac, d_offsets, d_P, d_Q);
+    M25_LAUNCH_CHECK("k_near_fill");
+    M25_CHECK(cudaStreamSynchronize(S(stream)));
+    return M25_OK;
+}
+
+extern "C" int m25_fan_q(const int *d_F, int nf, double *d_out, const m25_mesh *g, const m25_tables *tb, void *stream)
+{
+    M25_REQUIRE(g && tb, "m25_fan_q: null argument");
+    long tot = (long)g->Nt * nf;
+    if (!tot) return M25_OK;
+    k_fan_q<<<(tot + 255) / 256, 256, 0, S(stream)>>>(d_F, nf, d_out, *g, *tb);
+    M25_LAUNCH_CHECK("k_fan_q");
+    return M25_OK;
+}
+
+extern "C" int m25_radial_table_sum(const double *d_px, const double *d_py, const double *d_W, long nt, int nq,
+                                    const double *d_vx, const double *d_vy, int nv, const double *d_table, long n,
+                                    double dr, double *d_out, void *stream)
+{
+    M25_REQUIRE(n >= 2 && dr > 0, "m25_radial_table_sum: a table of two points or more, dr > 0");
+    long tot = nt * nv;
+    if (!tot) return M25_OK;
+    k_radial_table_sum<<<(tot + 255) / 256, 256, 0, S(stream)>>>(d_px, d_py, d_W, nt, nq, d_vx, d_vy, nv, d_table,
+                                                                  n, dr, d_out);
+    M25_LAUNCH_CHECK("k_radial_table_sum");
+    return M25_OK;
+}
+
+extern "C" int m25_matvec_far_multi(const double *d_X, int K, double *d_Y, double *d_work, const m25_mesh *g,
+                                    const m25_tables *tb, double w, void *stream)
+{
+    M25_REQUIRE(g && tb && d_X && d_Y && d_work, "m25_matvec_far_multi: null argument");
+    M25_REQUIRE(K >= 1 && K <= 16, "m25_matvec_far_multi: 1 <= K <= 16 columns a call");
+    size_t nk = (size_t)g->Nt * K * 2;
+    double *s0 = d_work, *s1x = s0 + nk, *s1y = s1x + nk, *vAx = s1y + nk, *vAy = vAx + nk, *wQ = vAy + nk;
+    long tot = (long)g->Nt * K;
+    k_mv_aggregate<<<(tot + 255) / 256, 256, 0, S(stream)>>>(d_X, K, *g, s0, s1x, s1y);
+    M25_LAUNCH_CHECK("k_mv_aggregate");
+    int blocks = (g->Nt + 127) / 128;
+    if (K <= 4)
+        k_mv_pairs<4><<<blocks, 128, 0, S(stream)>>>(K, *g, *tb, s0, s1x, s1y, vAx, vAy, wQ);
+    else if (K <= 8)
+        k_mv_pairs<8><<<blocks, 128, 0, S(stream)>>>(K, *g, *tb, s0, s1x, s1y, vAx, vAy, wQ);
+    else
+        k_mv_pairs<16><<<blocks, 128, 0, S(stream)>>>(K, *g, *tb, s0, s1x, s1y, vAx, vAy, wQ);
+    M25_LAUNCH_CHECK("k_mv_pairs");
+    tot = (long)g->Ne * K;
+    k_mv_finish<<<(tot + 255) / 256, 256, 0, S(stream)>>>(K, *g, w, vAx, vAy, wQ, d_Y);
+    M25_LAUNCH_CHECK("k_mv_finish");
+    return M25_OK;
+}
+
+extern "C" int m25_equilibrate(double *d_Z, long n, long ld, const double *d_d, double *d_dsc_out, float *d_Z64,
+                               void *stream)
+{
+    M25_REQUIRE(d_Z && ld >= n, "m25_equilibrate: Z and ld >= n");
+    const double *d = d_d;
+    if (d_dsc_out) {
+        k_diag_scale<<<(n + 255) / 256, 256, 0, S(stream)>>>(d_Z, n, ld, d_dsc_out);
+        M25_LAUNCH_CHECK("k_diag_scale");
+        d = d_dsc_out;
+    }
+    M25_REQUIRE(d, "m25_equilibrate: scales or an output for them");
+    dim3 grid((unsigned)std::min<long>((n + 255) / 256, 64), (unsigned)n);
+    k_equilibrate<<<grid, 256, 0, S(stream)>>>(d_Z, n, ld, d, d_Z64);
+    M25_LAUNCH_CHECK("k_equilibrate");
+    return M25_OK;
+}
+
+// the same for a complex64 Z (the mixed-precision path fills Z in complex64 directly): scales from its diagonal
+extern "C" int m25_equilibrate_c64(float *d_Z, long n, long ld, double *d_dsc_out, void *stream)
+{
+    M25_REQUIRE(d_Z && d_dsc_out && ld >= n, "m25_equilibrate_c64: Z, scales, ld >= n");
+    k_diag_scale_c64<<<(n + 255) / 256, 256, 0, S(stream)>>>(d_Z, n, ld, d_dsc_out);
+    M25_LAUNCH_CHECK("k_diag_scale_c64");
+    dim3 grid((unsigned)std::min<long>((n + 255) / 256, 64), (unsigned)n);
+    k_equilibrate_c64<<<grid, 256, 0, S(stream)>>>(d_Z, n, ld, d_dsc_out);
+    M25_LAUNCH_CHECK("k_equilibrate_c64");
+    return M25_OK;
+}

@@ -1,0 +1,197 @@
+// gmres.cu - the vector kernels of the mixed-precision refinement (mom25d fast.py:1437-1500 gmres_batched, run in
+// lockstep over k right-hand sides) and the pieces of the exact double-precision operator it iterates with
+// (fast.py:571-593 matvec_exact): the near-field COO product and the via border.
+// Vectors are N x k row-major complex128 (one column per right-hand side).
+#include "common.cuh"
+
+static inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+// out[c] = sum_n conj(V[n, c]) W[n, c]  (out zeroed by the caller; block partial sums added atomically)
+__global__ void k_dotc_cols(const double *V, const double *W, long N, int k, double *out)
+{
+    __shared__ double sx[16][33], sy[16][33];
+    double ax[16], ay[16];
+    for (int c = 0; c < 16; ++c) ax[c] = ay[c] = 0;
+    for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < k; ++c) {
+            zd v = ldc<double>(V, (size_t)n * k + c), w = ldc<double>(W, (size_t)n * k + c);
+            ax[c] += v.x * w.x + v.y * w.y;
+            ay[c] += v.x * w.y - v.y * w.x;
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int c = 0; c < k; ++c) {
+        double x = ax[c], y = ay[c];
+        for (int o = 16; o; o >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, o); y += __shfl_xor_sync(0xffffffffu, y, o); }
+        if (lane == 0) { sx[c][wid] = x; sy[c][wid] = y; }
+    }
+    __syncthreads();
+    if (threadIdx.x < k) {
+        double x = 0, y = 0;
+        for (int j = 0; j < (int)(blockDim.x / 32); ++j) { x += sx[threadIdx.x][j]; y += sy[threadIdx.x][j]; }
+        atomicAdd(out + 2 * threadIdx.x, x);
+        atomicAdd(out + 2 * threadIdx.x + 1, y);
+    }
+}
+
+// W[n, c] += V[n, c] a[c]   (a complex, per column)
+__global__ void k_axpy_cols(double *W, const double *V, const double *a, long N, int k)
+{
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= N * k) return;
+    int c = e % k;
+    zd w = ldc<double>(W, e);
+    cfma<double>(w, ldc<double>(V, e), ldc<double>(a, c));
+    stc<double>(W, e, w);
+}
+
+// Y[n, c] = X[n, c] s[c] (s complex per column) and, with d != NULL, times d[n] (a row scaling)
+__global__ void k_scale_cols(double *Y, const double *X, const double *s, const double *d, long N, int k)
+{
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= N * k) return;
+    int c = e % k;
+    long n = e / k;
+    zd x = ldc<double>(X, e);
+    if (s) x = x * ldc<double>(s, c);
+    if (d) x = x * d[n];
+    stc<double>(Y, e, x);
+}
+
+// complex128 <-> complex64 (the complex64 factor's solves)
+__global__ void k_z2c(const double *X, float *Y, long n)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) { Y[2 * i] = (float)X[2 * i]; Y[2 * i + 1] = (float)X[2 * i + 1]; }
+}
+__global__ void k_c2z(const float *X, double *Y, long n)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) { Y[2 * i] = X[2 * i]; Y[2 * i + 1] = X[2 * i + 1]; }
+}
+
+// Y[ri[s], c] += vv[s] X[ci[s], c] over the near field's COO triplets (ri < 0: unused)
+__global__ void k_coo_spmm(const int *ri, const int *ci, const double *vv, long nnz, const double *X, int k, double *Y)
+{
+    long s = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    int r = ri[s];
+    if (r < 0) return;
+    int cc = ci[s];
+    zd v = ldc<double>(vv, s);
+    for (int c = 0; c < k; ++c) {
+        zd y = v * ldc<double>(X, (size_t)cc * k + c);
+        atomicAdd(Y + 2 * ((size_t)r * k + c), y.x);
+        atomicAdd(Y + 2 * ((size_t)r * k + c) + 1, y.y);
+    }
+}
+
+// Z (complex64, ld) += vv at (ri, ci) (the near field into the mixed-precision matrix)
+__global__ void k_coo_add_c64(const int *ri, const int *ci, const double *vv, long nnz, float *Z, long ld)
+{
+    long s = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (s >= nnz) return;
+    int r = ri[s];
+    if (r < 0) return;
+    zd v = ldc<double>(vv, s);
+    size_t o = (size_t)r * ld + ci[s];
+    atomicAdd(Z + 2 * o, (float)v.x);
+    atomicAdd(Z + 2 * o + 1, (float)v.y);
+}
+
+// the via border of Z X (fast.py:580-586 _bordered): Y[:Ne] += B X[Ne:], Y[Ne:] = B^T X[:Ne] + C X[Ne:]
+// B: Ne x Nv, C: Nv x Nv row-major complex128
+__global__ void k_border_top(const double *B, int Ne, int Nv, const double *X, int k, double *Y)
+{
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= (long)Ne * k) return;
+    long r = e / k;
+    int c = e % k;
+    zd acc = ldc<double>(Y, e);
+    for (int n = 0; n < Nv; ++n) cfma<double>(acc, ldc<double>(B, (size_t)r * Nv + n), ldc<double>(X, (size_t)(Ne + n) * k + c));
+    stc<double>(Y, e, acc);
+}
+__global__ void k_border_bottom(const double *B, const double *C, int Ne, int Nv, const double *X, int k, double *Y)
+{
+    // one block per (n, c): B^T X over the Ne edges, reduced in the block
+    int n = blockIdx.x / k, c = blockIdx.x % k;
+    zd acc = mk<double>(0, 0);
+    for (long e = threadIdx.x; e < Ne; e += blockDim.x) cfma<double>(acc, ldc<double>(B, (size_t)e * Nv + n), ldc<double>(X, (size_t)e * k + c));
+    __shared__ double sx[32], sy[32];
+    double x = acc.x, y = acc.y;
+    for (int o = 16; o; o >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, o); y += __shfl_xor_sync(0xffffffffu, y, o); }
+    if ((threadIdx.x & 31) == 0) { sx[threadIdx.x >> 5] = x; sy[threadIdx.x >> 5] = y; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        zd t = mk<double>(0, 0);
+        for (int j = 0; j < (int)(blockDim.x / 32); ++j) t += mk<double>(sx[j], sy[j]);
+        for (int m = 0; m < Nv; ++m) cfma<double>(t, ldc<double>(C, (size_t)n * Nv + m), ldc<double>(X, (size_t)(Ne + m) * k + c));
+        stc<double>(Y, (size_t)(Ne + n) * k + c, t);
+    }
+}
+
+// ======================================================================================================================
+extern "C" int m25_dotc_cols(const double *d_V, const double *d_W, long N, int k, double *d_out, void *stream)
+{
+    M25_REQUIRE(k >= 1 && k <= 16, "m25_dotc_cols: 1 to 16 columns");
+    M25_CHECK(cudaMemsetAsync(d_out, 0, sizeof(double) * 2 * k, S(stream)));
+    int blocks = (int)std::min<long>(592, (N + 255) / 256);
+    k_dotc_cols<<<blocks, 256, 0, S(stream)>>>(d_V, d_W, N, k, d_out);
+    M25_LAUNCH_CHECK("k_dotc_cols");
+    return M25_OK;
+}
+
+extern "C" int m25_axpy_cols(double *d_W, const double *d_V, const double *d_a, long N, int k, void *stream)
+{
+    long t = N * k;
+    k_axpy_cols<<<(t + 255) / 256, 256, 0, S(stream)>>>(d_W, d_V, d_a, N, k);
+    M25_LAUNCH_CHECK("k_axpy_cols");
+    return M25_OK;
+}
+
+extern "C" int m25_scale_cols(double *d_Y, const double *d_X, const double *d_s, const double *d_rows, long N, int k,
+                              void *stream)
+{
+    long t = N * k;
+    k_scale_cols<<<(t + 255) / 256, 256, 0, S(stream)>>>(d_Y, d_X, d_s, d_rows, N, k);
+    M25_LAUNCH_CHECK("k_scale_cols");
+    return M25_OK;
+}
+
+extern "C" int m25_convert(const void *d_in, int in_single, void *d_out, long n, void *stream)
+{
+    if (!n) return M25_OK;
+    if (in_single) k_c2z<<<(n + 255) / 256, 256, 0, S(stream)>>>((const float *)d_in, (double *)d_out, n);
+    else k_z2c<<<(n + 255) / 256, 256, 0, S(stream)>>>((const double *)d_in, (float *)d_out, n);
+    M25_LAUNCH_CHECK("k_convert");
+    return M25_OK;
+}
+
+extern "C" int m25_coo_spmm(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, const double *d_X, int k,
+                            double *d_Y, void *stream)
+{
+    if (!nnz) return M25_OK;
+    k_coo_spmm<<<(nnz + 255) / 256, 256, 0, S(stream)>>>(d_ri, d_ci, d_vv, nnz, d_X, k, d_Y);
+    M25_LAUNCH_CHECK("k_coo_spmm");
+    return M25_OK;
+}
+
+extern "C" int m25_coo_add_c64(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, float *d_Z, long ld,
+                               void *stream)
+{
+    if (!nnz) return M25_OK;
+    k_coo_add_c64<<<(nnz + 255) / 256, 256, 0, S(stream)>>>(d_ri, d_ci, d_vv, nnz, d_Z, ld);
+    M25_LAUNCH_CHECK("k_coo_add_c64");
+    return M25_OK;
+}
+
+extern "C" int m25_border_mv(const double *d_B, const double *d_C, int Ne, int Nv, const double *d_X, int k,
+                             double *d_Y, void *stream)
+{
+    if (!Nv) return M25_OK;
+    long t = (long)Ne * k;
+    k_border_top<<<(t + 255) / 256, 256, 0, S(stream)>>>(d_B, Ne, Nv, d_X, k, d_Y);
+    M25_LAUNCH_CHECK("k_border_top");
+    k_border_bottom<<<Nv * k, 256, 0, S(stream)>>>(d_B, d_C, Ne, Nv, d_X, k, d_Y);
+    M25_LAUNCH_CHECK("k_border_bottom");
+    return M25_OK;
+}

@@ -1,0 +1,289 @@
+"""
+mom25d_b200.operator - the direct solver of one board on the GPU: the drop-in for the reference's
+FastOperator.solve_direct (mom25d fast.py:704-850) behind the same call, solve_direct(f, E, block, precision).
+
+  precision='double'  complex128 Green tables, fill, near correction and via border into a device Z; symmetric
+                      equilibration; complex128 LU with partial pivoting; the triangular solves. Matches the
+                      reference's complex128 fill and LAPACK solve.
+  precision='mixed'   complex64 fill from complex64 tables, the near field's double-precision triplets added; LU in
+                      complex64 (trailing updates 3xTF32 on the tensor cores when tf32=True); refined by batched
+                      GMRES (fast.py:1437-1500) on the EXACT double-precision operator applied without a matrix:
+                      the triangle-aggregated far field (matvec_far_multi), the near field's triplets and the via
+                      border (fast.py:571-593). The refinement's residuals and corrections are double precision.
+
+Every step runs in libmom25d_b200 kernels; the host runs the GMRES recurrences on k x restart scalars.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import P, check, lib, stream_ptr
+from .device import DeviceGeometry, DeviceTables, DeviceVias
+
+c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
+MIXED_MAX_ITER = 30          # fast.py:255
+FRESH_STALL = (4, 0.1)       # fast.py:256
+MIXED_RTOL = 1e-6            # fast.py:366 (FastOperator.mixed_tol)
+
+
+class SolveFailed(RuntimeError):
+    """The mixed-precision refinement did not converge (the caller redoes the frequency in double)."""
+
+
+class DirectSolver:
+    """One board's device-resident direct solver (meshes, pairs, tables and factors stay on the GPU)."""
+
+    def __init__(self, geo, stream=None, tf32=False, log=None):
+        self.geo, self.stream = geo, stream
+        self.dg = DeviceGeometry(geo, stream)
+        self.tf32 = tf32
+        self.log = log if log is not None else []
+        self.timings = {}
+        self.iters = []
+        self._work = {}
+
+    # ---- buffers kept across frequencies ---------------------------------------------------------------------------
+    def _buf(self, name, shape, dtype):
+        t = self._work.get(name)
+        if t is None or t.shape != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device='cuda')
+            self._work[name] = t
+        return t
+
+    def _getrf_work(self, n, single):
+        nbytes = int(lib().m25_getrf_workspace(c_int(n), c_int(1 if single else 0)))
+        return self._buf('getrf_work_%d' % single, (nbytes,), torch.uint8)
+
+    @property
+    def s(self):
+        return stream_ptr(self.stream)
+
+    def _t(self, name, t0):
+        torch.cuda.current_stream().synchronize() if self.stream is None else self.stream.synchronize()
+        self.timings[name] = self.timings.get(name, 0.0) + time.perf_counter() - t0
+
+    # ---- tables and fill -----------------------------------------------------------------------------------------
+    def setup(self, f, single=False):
+        self.f, self.w = f, 2 * np.pi * f
+        self.tabs = DeviceTables(self.dg, f, single=single, stream=self.stream)
+        self.vias = DeviceVias(self.dg, self.tabs, self.stream)
+
+    def impedance(self, f, precision='double'):
+        """Z at f on the device: complex128 (double) or complex64 (mixed)."""
+        geo, dg = self.geo, self.dg
+        N, Ne = geo.N, geo.Ne
+        single = precision == 'mixed'
+        self.setup(f, single=single)
+        tb, s = self.tabs, self.s
+        qcorr = self._buf('qcorr', (max(1, dg.npairs),), torch.complex128)
+        if not single:
+            Z = self._buf('Z', (N, N), torch.complex128)
+            check(lib().m25_fill_far(P(Z), c_long(N), c_int(0), ctypes.byref(dg.mesh), ctypes.byref(tb.tables), None,
+                                     c_double(self.w), s), 'm25_fill_far')
+            check(lib().m25_near(c_int(0), P(Z), c_long(N), c_int(0), None, None, None, P(qcorr), P(dg.stat),
+                                 c_int(int(dg.stat_ready)), ctypes.byref(dg.mesh), ctypes.byref(tb.tables),
+                                 ctypes.byref(dg.quad), P(dg.nP), P(dg.nQ), c_long(dg.npairs), c_double(self.w), s),
+                  'm25_near')
+            dg.stat_ready = True
+            self.vias.assemble(Z, N, qcorr)
+            return Z
+        Z = self._buf('Z64', (N, N), torch.complex64)
+        check(lib().m25_fill_far(P(Z), c_long(N), c_int(1), ctypes.byref(dg.mesh), None, ctypes.byref(tb.tables32),
+                                 c_double(self.w), s), 'm25_fill_far')
+        nnz = 9 * dg.npairs
+        self.ri = self._buf('ri', (max(1, nnz),), torch.int32)
+        self.ci = self._buf('ci', (max(1, nnz),), torch.int32)
+        self.vv = self._buf('vv', (max(1, nnz),), torch.complex128)
+        check(lib().m25_near(c_int(2), None, c_long(0), c_int(0), P(self.ri), P(self.ci), P(self.vv), P(qcorr),
+                             P(dg.stat), c_int(int(dg.stat_ready)), ctypes.byref(dg.mesh), ctypes.byref(tb.tables),
+                             ctypes.byref(dg.quad), P(dg.nP), P(dg.nQ), c_long(dg.npairs), c_double(self.w), s),
+              'm25_near')
+        dg.stat_ready = True
+        check(lib().m25_coo_add_c64(P(self.ri), P(self.ci), P(self.vv), c_long(nnz), P(Z), c_long(N), s),
+              'm25_coo_add_c64')
+        self.Bv = self._buf('Bv', (max(1, Ne * geo.Nv),), torch.complex128)
+        self.Cv = self._buf('Cv', (max(1, geo.Nv * geo.Nv),), torch.complex128)
+        self.vias.assemble(None, N, qcorr, Z64=Z, B=self.Bv, C=self.Cv)
+        return Z
+
+    # ---- the exact double-precision operator (fast.py:571-593) --------------------------------------------------------
+    def matvec_exact(self, X):
+        """Z X in double precision without Z: X (N x k) complex128 device tensor -> new tensor."""
+        geo, dg, s = self.geo, self.dg, self.s
+        N, Ne, k = geo.N, geo.Ne, X.shape[1]
+        X = X.contiguous()
+        Y = torch.empty_like(X)
+        Xe = X[:Ne].contiguous()
+        work = self._buf('mv_work', (6 * geo.Nt * k,), torch.complex128)
+        Ye = torch.empty((Ne, k), dtype=torch.complex128, device='cuda')
+        check(lib().m25_matvec_far_multi(P(Xe), c_int(k), P(Ye), P(work), ctypes.byref(dg.mesh),
+                                         ctypes.byref(self.tabs.tables), c_double(self.w), s), 'm25_matvec_far_multi')
+        check(lib().m25_coo_spmm(P(self.ri), P(self.ci), P(self.vv), c_long(9 * dg.npairs), P(Xe), c_int(k), P(Ye), s),
+              'm25_coo_spmm')
+        Y[:Ne] = Ye
+        if geo.Nv:
+            check(lib().m25_border_mv(P(self.Bv), P(self.Cv), c_int(Ne), c_int(geo.Nv), P(X), c_int(k), P(Y), s),
+                  'm25_border_mv')
+        return Y
+
+    # ---- device vector helpers ------------------------------------------------------------------------------------------
+    def _dotc(self, V, W):
+        k = V.shape[1]
+        out = self._buf('dot', (k,), torch.complex128)
+        check(lib().m25_dotc_cols(P(V), P(W), c_long(V.shape[0]), c_int(k), P(out), self.s), 'm25_dotc_cols')
+        return out.cpu().numpy().copy()
+
+    def _axpy(self, W, V, a):
+        a_d = _lib.dev(np.asarray(a, complex))
+        check(lib().m25_axpy_cols(P(W), P(V), P(a_d), c_long(W.shape[0]), c_int(W.shape[1]), self.s), 'm25_axpy_cols')
+
+    def _scale(self, X, s_cols=None, rows=None, out=None):
+        Y = torch.empty_like(X) if out is None else out
+        sc = None if s_cols is None else _lib.dev(np.asarray(s_cols, complex))
+        check(lib().m25_scale_cols(P(Y), P(X), P(sc), P(rows), c_long(X.shape[0]), c_int(X.shape[1]), self.s),
+              'm25_scale_cols')
+        return Y
+
+    # ---- solves -------------------------------------------------------------------------------------------------------
+    def _factor(self, Z, single):
+        N = self.geo.N
+        ipiv = self._buf('ipiv', (N,), torch.int32)
+        work = self._getrf_work(N, single)
+        check(lib().m25_getrf(P(Z), c_long(N), c_int(N), P(ipiv), c_int(int(single)),
+                              c_int(int(single and self.tf32)), P(work), ctypes.c_size_t(work.numel()), self.s),
+              'm25_getrf')
+        _lib.sync_check(self.stream, 'm25_getrf')
+        return ipiv
+
+    def _lu_solve(self, Z, ipiv, R, single):
+        """Z^-1 R with the factor (lu_solve(..., trans=1)), R complex128 (N x k) -> complex128."""
+        N, k = R.shape
+        if single:
+            R64 = torch.empty((N, k), dtype=torch.complex64, device='cuda')
+            check(lib().m25_convert(P(R), c_int(0), P(R64), c_long(N * k), self.s), 'm25_convert')
+            check(lib().m25_getrs(P(Z), c_long(N), c_int(N), P(ipiv), c_int(1), P(R64), c_int(k), self.s), 'm25_getrs')
+            X = torch.empty((N, k), dtype=torch.complex128, device='cuda')
+            check(lib().m25_convert(P(R64), c_int(1), P(X), c_long(N * k), self.s), 'm25_convert')
+            return X
+        X = R.clone()
+        check(lib().m25_getrs(P(Z), c_long(N), c_int(N), P(ipiv), c_int(0), P(X), c_int(k), self.s), 'm25_getrs')
+        return X
+
+    def solve_direct(self, f, E, block=1024, precision='double'):
+        """Currents for the excitation columns E (N x k, host or device): a complex128 device tensor."""
+        geo = self.geo
+        N = geo.N
+        E = torch.as_tensor(np.asarray(E) if not torch.is_tensor(E) else E, dtype=torch.complex128).to('cuda')
+        E = E.reshape(N, -1).contiguous()
+        self.iters = []
+        single = precision == 'mixed'
+        t0 = time.perf_counter()
+        Z = self.impedance(f, precision)
+        self._t('fill', t0)
+        dsc = self._buf('dsc', (N,), torch.float64)
+        t0 = time.perf_counter()
+        if single:
+            check(lib().m25_equilibrate_c64(P(Z), c_long(N), c_long(N), P(dsc), self.s), 'm25_equilibrate_c64')
+        else:
+            check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
+        ipiv = self._factor(Z, single)
+        self._t('lu', t0)
+        t0 = time.perf_counter()
+        B = self._scale(E, rows=dsc)
+        if not single:
+            Y = self._lu_solve(Z, ipiv, B, False)
+            X = self._scale(Y, rows=dsc)
+            self._t('solve', t0)
+            return X
+        A = lambda V: self._scale(self.matvec_exact(self._scale(V, rows=dsc)), rows=dsc)
+        M = lambda R: self._lu_solve(Z, ipiv, R, True)
+        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, 1, FRESH_STALL)
+        self._t('refine', t0)
+        if not ok:
+            raise SolveFailed(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e})")
+        return self._scale(Y, rows=dsc)
+
+    def refine(self, A, B, M, restart, maxiter, stall=None):
+        """fast.py:658-663: batched GMRES to MIXED_RTOL; (Y, converged, largest relative residual)."""
+        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, maxiter=maxiter, stall=stall)
+        R = B - A(Y)
+        rn = np.sqrt(np.abs(self._dotc(R, R)))
+        bn = np.sqrt(np.abs(self._dotc(B, B)))
+        rel = rn / np.maximum(bn, 1e-300)
+        self.residual = rel
+        return Y, bool(np.isfinite(rel).all() and (rel <= 100 * MIXED_RTOL).all()), float(rel.max())
+
+    def gmres_batched(self, A, B, M=None, rtol=1e-6, restart=30, maxiter=10, stall=None):
+        """fast.py:1437-1500 on device vectors: right-preconditioned restarted GMRES for k systems in lockstep,
+        modified Gram-Schmidt, conjugated Givens rotations, the stall rule. The (restart x restart) Hessenberg
+        recurrences run on the host."""
+        N, k = B.shape
+        X = torch.zeros_like(B)
+        M = M or (lambda R: R.clone())
+        bn = np.sqrt(np.abs(self._dotc(B, B)))
+        bn[bn == 0] = 1.0
+        iters, act = np.zeros(k, int), np.arange(k)
+        started = False
+        for _ in range(maxiter):
+            Xa = X[:, act].contiguous()
+            R = B[:, act].contiguous()
+            if started:
+                R = R - A(Xa)
+            beta = np.sqrt(np.abs(self._dotc(R, R)))
+            done = beta <= rtol * bn[act]
+            keep = np.flatnonzero(~done)
+            act, beta = act[keep], beta[keep]
+            if not len(act):
+                break
+            R = R[:, torch.as_tensor(keep, device='cuda')].contiguous()
+            ka = len(act)
+            V, Zk = [None] * (restart + 1), [None] * restart
+            H = np.zeros((restart + 1, restart, ka), complex)
+            g = np.zeros((restart + 1, ka), complex)
+            cs, sn = np.zeros((restart, ka), complex), np.zeros((restart, ka), complex)
+            g[0] = beta
+            V[0] = self._scale(R, s_cols=1.0 / beta)
+            live, last, stalled = np.ones(ka, bool), np.full(ka, restart - 1), False
+            for j in range(restart):
+                Zk[j] = M(V[j])
+                Wv = A(Zk[j])
+                for i in range(j + 1):
+                    hij = self._dotc(V[i], Wv)
+                    H[i, j] = hij
+                    self._axpy(Wv, V[i], -hij)
+                hn = np.sqrt(np.abs(self._dotc(Wv, Wv)))
+                H[j + 1, j] = hn
+                V[j + 1] = self._scale(Wv, s_cols=1.0 / np.where(hn > 0, hn, 1))
+                for i in range(j):
+                    H[i, j], H[i + 1, j] = (cs[i] * H[i, j] + sn[i] * H[i + 1, j],
+                                            -np.conj(sn[i]) * H[i, j] + np.conj(cs[i]) * H[i + 1, j])
+                den = np.sqrt(np.abs(H[j, j]) ** 2 + np.abs(H[j + 1, j]) ** 2)
+                den[den == 0] = 1.0
+                cs[j], sn[j] = H[j, j].conj() / den, H[j + 1, j].conj() / den
+                H[j, j], H[j + 1, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j], 0
+                g[j + 1], g[j] = -np.conj(sn[j]) * g[j], cs[j] * g[j]
+                iters[act[live]] += 1
+                conv = live & (np.abs(g[j + 1]) <= rtol * bn[act])
+                last[conv] = j
+                live &= ~conv
+                if not live.any():
+                    break
+                if stall is not None and j + 1 >= stall[0] and (np.abs(g[j + 1])[live] > stall[1] * bn[act][live]).any():
+                    last[live], stalled = j, True
+                    break
+            ys = []
+            for c in range(ka):
+                m = last[c] + 1
+                ys.append(np.linalg.solve(np.triu(H[:m, :m, c]), g[:m, c]) if m else np.zeros(0))
+            Xa = X[:, act].contiguous()
+            for j in range(max(last) + 1):
+                a = np.array([ys[c][j] if j < len(ys[c]) else 0.0 for c in range(ka)], complex)
+                self._axpy(Xa, Zk[j], a)
+            X[:, torch.as_tensor(act, device='cuda')] = Xa
+            started = True
+            if stalled:
+                break
+        return X, iters.tolist()

@@ -1,0 +1,211 @@
+"""Parity of the CUDA hot path with the oracle (a CPU restatement of the reference, pinned in test_oracle.py) and
+with the golden fixtures the reference itself wrote. All through the C ABI (libmom25d_b200.so)."""
+import ctypes
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+import oracle
+from oracle import green, solve as osolve
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip('torch')
+
+
+def _small_board():
+    from mom25d_b200 import board as B
+    spec = importlib.util.spec_from_file_location('mg', os.path.join(os.path.dirname(__file__), 'golden',
+                                                                     'make_golden.py'))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.small_board(B)
+
+
+@pytest.fixture(scope='module')
+def small():
+    from mom25d_b200 import geometry as G
+    from mom25d_b200.operator import DirectSolver
+    geo = G.Geometry(_small_board())
+    return geo, DirectSolver(geo), osolve.Direct(geo)
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+def upload_tables(tb):
+    """The oracle's tb dictionary as device tables (the kernels alone, without the table builder)."""
+    from mom25d_b200 import _lib
+    d = {k: _lib.dev(tb[k], np.int32 if k in ('tab', 'kind') else (np.float64 if k in ('dr', 'd', 'dimg') else
+                                                                    np.complex128)) for k in tb}
+    T = _lib.Tables(tb['A'].shape[0], tb['A'].shape[1], len(tb['tab']),
+                    *[_lib.P(d[k]) for k in ('A', 'Q', 'cA', 'cq', 'cAi', 'cqi', 'dr', 'd', 'dimg', 'tab', 'kind')])
+    return T, d
+
+
+def test_near_pairs_match(small):
+    geo, ds, od = small
+    n = ds.dg.npairs
+    assert np.array_equal(ds.dg.nP[:n].cpu().numpy(), od.nP) and np.array_equal(ds.dg.nQ[:n].cpu().numpy(), od.nQ)
+
+
+@pytest.mark.parametrize('f', [0.5e9, 3.0e9, 10e9])
+def test_green_tables_match(small, f):
+    from mom25d_b200.device import DeviceTables
+    geo, ds, od = small
+    od.setup(f)
+    dt = DeviceTables(ds.dg, f, single=True)
+    hd = dt.host_dict(geo)
+    # The image coefficients come from the network's large-kr limit times exp(18) (multilayer.py:279-285): their
+    # last digits depend on the libm in use, and the tables absorb the difference. What the fill uses is the total
+    # kernel A_rest + sum c / sqrt(rho^2 + d^2): that is compared (at rho > 0), and the coefficients loosely.
+    rho = np.linspace(0, geo.rho_max, 8192)[1:]
+    for t in range(len(hd['kind'])):
+        for k, c, ci in (('A', 'cA', 'cAi'), ('Q', 'cq', 'cqi')):
+            tot = lambda h: (h[k][t][1:] + (h[c][t] / rho if h['kind'][t] == 0 else
+                                             h[c][t] / np.hypot(rho, h['d'][t]) if h['kind'][t] == 1 else 0)
+                             + (h[ci][t] / np.hypot(rho, h['dimg'][t]) if h['dimg'][t] > 0 else 0))
+            assert rel(tot(hd), tot(od.tb)) < 1e-11, (t, k)
+    for k in ('cA', 'cq', 'd', 'dimg', 'dr'):
+        assert np.allclose(hd[k], od.tb[k], rtol=1e-12, atol=0), k
+    for k in ('cAi', 'cqi'):
+        assert np.allclose(hd[k], od.tb[k], rtol=1e-6, atol=0), k
+    assert np.array_equal(hd['kind'], od.tb['kind'])
+    # the mixed fill's complex64 tables: the same spline on 4096 points, rounded
+    A32 = dt.AQ32.cpu().numpy()
+    n = len(hd['kind'])
+    rho32 = np.linspace(0, geo.rho_max, 4096)
+    from scipy.interpolate import CubicSpline
+    H = dt.H.cpu().numpy()
+    for i in range(n):
+        want = CubicSpline(ds.dg.rho_coarse, H[i])(rho32)
+        assert np.abs(A32[i] - want).max() <= 1e-6 * np.abs(want).max()
+
+
+def test_fill_far_and_near_kernels_match_the_oracle(small):
+    from mom25d_b200 import _lib
+    geo, ds, od = small
+    f = 3e9
+    od.setup(f)
+    T, keep = upload_tables(od.tb)
+    Ne, w = geo.Ne, 2 * np.pi * f
+    Z = torch.zeros((Ne, Ne), dtype=torch.complex128, device='cuda')
+    _lib.check(_lib.lib().m25_fill_far(_lib.P(Z), ctypes.c_long(Ne), 0, ctypes.byref(ds.dg.mesh), ctypes.byref(T),
+                                       None, ctypes.c_double(w), _lib.stream_ptr()))
+    Zo = np.zeros((Ne, Ne), complex)
+    oracle.fill_far(Zo, geo.g, od.tb, w)
+    Zg = Z.cpu().numpy()
+    assert rel(Zg, Zo) < 1e-13
+    assert np.array_equal(Zg, Zg.T)                               # written symmetric, as the reference does
+    qc = torch.zeros(ds.dg.npairs, dtype=torch.complex128, device='cuda')
+    stat = torch.zeros(12 * ds.dg.npairs, dtype=torch.float64, device='cuda')
+    for ready in (0, 1):                                          # computes, then reuses the analytic parts
+        Zr = Z.clone()
+        _lib.check(_lib.lib().m25_near(0, _lib.P(Zr), ctypes.c_long(Ne), 0, None, None, None, _lib.P(qc), _lib.P(stat),
+                                       ready, ctypes.byref(ds.dg.mesh), ctypes.byref(T), ctypes.byref(ds.dg.quad),
+                                       _lib.P(ds.dg.nP), _lib.P(ds.dg.nQ), ctypes.c_long(ds.dg.npairs),
+                                       ctypes.c_double(w), _lib.stream_ptr()))
+        _lib.sync_check()
+        Zn = Zo.copy()
+        qo = oracle.near_into_dense(Zn, geo.g, od.tb, geo.q, od.nP32, od.nQ32, w)
+        assert rel(Zr.cpu().numpy(), Zn) < 1e-12
+        assert rel(qc.cpu().numpy(), qo) < 1e-12
+    # COO triplets
+    n9 = 9 * ds.dg.npairs
+    ri = torch.empty(n9, dtype=torch.int32, device='cuda'); ci = torch.empty_like(ri)
+    vv = torch.empty(n9, dtype=torch.complex128, device='cuda')
+    _lib.check(_lib.lib().m25_near(2, None, ctypes.c_long(0), 0, _lib.P(ri), _lib.P(ci), _lib.P(vv), _lib.P(qc),
+                                   _lib.P(stat), 1, ctypes.byref(ds.dg.mesh), ctypes.byref(T), ctypes.byref(ds.dg.quad),
+                                   _lib.P(ds.dg.nP), _lib.P(ds.dg.nQ), ctypes.c_long(ds.dg.npairs), ctypes.c_double(w),
+                                   _lib.stream_ptr()))
+    r1, c1, v1, _ = oracle.near_coo(geo.g, od.tb, geo.q, od.nP32, od.nQ32, w)
+    rg = ri.cpu().numpy()
+    assert np.array_equal(rg, r1)
+    ok = r1 >= 0
+    assert np.array_equal(ci.cpu().numpy()[ok], c1[ok])
+    assert np.abs(vv.cpu().numpy()[ok] - v1[ok]).max() <= 1e-12 * np.abs(v1[ok]).max()
+    # matrix-free far product
+    X = np.random.default_rng(0).normal(size=(Ne, 3)) + 1j * np.random.default_rng(1).normal(size=(Ne, 3))
+    Xd = _lib.dev(X, np.complex128)
+    Yd = torch.empty_like(Xd)
+    work = torch.empty(6 * geo.Nt * 3, dtype=torch.complex128, device='cuda')
+    _lib.check(_lib.lib().m25_matvec_far_multi(_lib.P(Xd), 3, _lib.P(Yd), _lib.P(work), ctypes.byref(ds.dg.mesh),
+                                               ctypes.byref(T), ctypes.c_double(w), _lib.stream_ptr()))
+    Yo = oracle.matvec_far_multi(X, geo.g, od.tb, w)
+    assert rel(Yd.cpu().numpy(), Yo) < 1e-12
+    assert rel(Yo, Zo @ X) < 1e-12                               # (the product is the far field's)
+
+
+def test_impedance_matches_the_reference(small, golden):
+    geo, ds, od = small
+    f = float(golden['board_f'][0])
+    Z = ds.impedance(f, 'double').cpu().numpy()
+    Zr = golden['board_Z']
+    assert rel(Z, Zr) <= 1e-10                                    # the drop-in bar: Z to 1e-10 (Frobenius)
+    Zo = od.impedance(f)
+    assert rel(Z, Zo) <= 1e-10
+
+
+def test_direct_solve_matches_the_reference(small, golden):
+    geo, ds, od = small
+    f = float(golden['board_f'][0])
+    X = ds.solve_direct(f, geo.excitation(), precision='double').cpu().numpy()
+    S = geo.sparams_from_currents(X)
+    assert np.abs(S - golden['board_S_double']).max() <= 1e-8      # the drop-in bar: max |dS| 1e-8
+    assert np.abs(X - golden['board_I_double']).max() <= 1e-8 * np.abs(golden['board_I_double']).max()
+
+
+def test_mixed_solve_matches_the_reference(small, golden):
+    geo, ds, od = small
+    f = float(golden['board_f'][0])
+    X = ds.solve_direct(f, geo.excitation(), precision='mixed').cpu().numpy()
+    S = geo.sparams_from_currents(X)
+    assert np.abs(S - golden['board_S_double']).max() <= 1e-4      # the mixed-precision bar
+    assert np.abs(S - golden['board_S_double']).max() <= 1e-5      # (refined to 1e-6: well inside it)
+    assert max(ds.iters) <= 30
+
+
+@pytest.mark.parametrize('single', [0, 1])
+@pytest.mark.parametrize('n', [300, 1000])
+def test_lu_matches_lapack(single, n):
+    """The LU against LAPACK (SciPy's lu_factor of Z^T): the same pivots, the factor to round-off, the solves
+    (the reference's own LU test, test_gpu.py:210-235: N = 300, + 4 sqrt(N) I, rows 0 and 7 interchanged)."""
+    from mom25d_b200 import _lib
+    rng = np.random.default_rng(3)
+    dt = np.complex64 if single else np.complex128
+    Z = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(dt)
+    Z += (4 * np.sqrt(n) * np.eye(n)).astype(dt)
+    Z[[0, 7]] = Z[[7, 0]]
+    Zd = _lib.dev(Z)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(_lib.lib().m25_getrf_workspace(n, single))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    _lib.check(_lib.lib().m25_getrf(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, 0, _lib.P(work),
+                                    ctypes.c_size_t(nb), _lib.stream_ptr()))
+    _lib.sync_check()
+    lu_ref, piv_ref = sla.lu_factor(Z.T.astype(complex))
+    lu = Zd.cpu().numpy().T                                         # the factor of Z^T (column-major in memory)
+    assert np.array_equal(ipiv.cpu().numpy(), piv_ref)
+    tol = 1e-4 if single else 1e-12
+    assert np.abs(lu - lu_ref).max() < tol * np.abs(lu_ref).max()
+    R = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
+    x = np.linalg.solve(Z.astype(complex), R)
+    Rd = _lib.dev(R.astype(dt))
+    _lib.check(_lib.lib().m25_getrs(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, _lib.P(Rd), 3,
+                                    _lib.stream_ptr()))
+    assert np.abs(Rd.cpu().numpy() - x).max() < (1e-4 if single else 1e-11) * np.abs(x).max()
+
+
+def test_complex_bessel_matches_the_reference(golden):
+    from mom25d_b200 import _lib
+    z = _lib.dev(golden['jn_z'], np.complex128)
+    out = torch.empty_like(z)
+    for n in range(3):
+        _lib.check(_lib.lib().m25_bessel_jn_complex(n, _lib.P(z), ctypes.c_long(z.numel()), _lib.P(out),
+                                                    _lib.stream_ptr()))
+        ref = golden['jn_%d' % n]
+        assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
