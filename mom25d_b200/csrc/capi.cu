@@ -6,7 +6,15 @@
 
 #include "common.cuh"
 
+#include <atomic>
+
 static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+void m25_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+// The number of kernels this library has launched since it was loaded (every launch site counts itself).
+extern "C" long long m25_launch_count(void) { return g_launches.load(); }
 
 void m25_set_error(const std::string &msg) { g_err = msg; }
 

@@ -66,6 +66,7 @@ template <typename R> __device__ __forceinline__ void stc(R *p, size_t i, cpx<R>
 // ---- error plumbing ---------------------------------------------------------------------------------------------------
 void m25_set_error(const std::string &msg);
 int m25_cuda_status(cudaError_t e, const char *where);
+void m25_note_launch();          // counts this library's kernel launches (m25_launch_count)
 #define M25_CHECK(call)                                                                                    \
     do {                                                                                                   \
         cudaError_t e_ = (call);                                                                           \
@@ -73,6 +74,7 @@ int m25_cuda_status(cudaError_t e, const char *where);
     } while (0)
 #define M25_LAUNCH_CHECK(what)                                                                             \
     do {                                                                                                   \
+        m25_note_launch();                                                                                 \
         cudaError_t e_ = cudaGetLastError();                                                               \
         if (e_ != cudaSuccess) return m25_cuda_status(e_, what);                                           \
     } while (0)

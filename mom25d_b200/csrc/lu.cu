@@ -23,6 +23,7 @@ int m25_umma_trailing(float *A, long lda, int M, int Ncol, int K, const float *L
 size_t m25_umma_workspace(int n, int nb);
 
 #define NB 64
+#define NB2 256
 #define PANEL_THREADS 256
 
 struct PanelWork {
@@ -33,6 +34,122 @@ struct PanelWork {
     GridBarrier bar;
 };
 
+// The panel with each block's rows held in shared memory for the whole panel (Ps[c * cs + i], row r0 + i): the
+// per-column work is shared-memory bound and parallel over (row, column); global memory is read once and written
+// once. Used whenever the rows fit (cs * jb * sizeof(complex) <= the opt-in shared memory).
+template <typename R>
+__global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, int n, int k0, int jb, int *ipiv,
+                                                              PanelWork pw, int *err)
+{
+    typedef cpx<R> C;
+    extern __shared__ unsigned char panel_raw[];
+    C *Ps = reinterpret_cast<C *>(panel_raw);
+    const unsigned G = gridDim.x;
+    const int b = blockIdx.x, tid = threadIdx.x;
+    const int rows = n - k0;
+    const int cs = (rows + G - 1) / G;
+    const int r0 = k0 + b * cs, r1 = min(n, r0 + cs);
+    const int nr = max(0, r1 - r0);
+    unsigned phase = 0;
+    __shared__ C U[NB], D[NB];
+    __shared__ double sv[PANEL_THREADS / 32];
+    __shared__ int si[PANEL_THREADS / 32];
+    __shared__ int s_p;
+    __shared__ C s_recip;
+    C *cand_row = reinterpret_cast<C *>(pw.cand_row);
+    C *drow = reinterpret_cast<C *>(pw.drow);
+    for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
+        int c = e / nr, i = e % nr;
+        Ps[c * cs + i] = ldc<R>(A, (size_t)(k0 + c) * lda + r0 + i);
+    }
+    __syncthreads();
+    for (int j = 0; j < jb; ++j) {
+        const int col = k0 + j, par = j & 1;
+        double best = -1.0;
+        int bi = 0x7fffffff;
+        for (int i = max(0, col - r0) + tid; i < nr; i += PANEL_THREADS) {
+            double v = abs1(Ps[j * cs + i]);
+            if (v > best) { best = v; bi = r0 + i; }
+        }
+        for (int o = 16; o; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if ((tid & 31) == 0) { sv[tid >> 5] = best; si[tid >> 5] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < PANEL_THREADS / 32; ++w)
+                if (sv[w] > best || (sv[w] == best && si[w] < bi)) { best = sv[w]; bi = si[w]; }
+            pw.cand_val[par * G + b] = best;
+            pw.cand_idx[par * G + b] = bi;
+            s_p = bi;
+        }
+        __syncthreads();
+        if (s_p != 0x7fffffff && tid < jb) cand_row[((size_t)par * G + b) * NB + tid] = Ps[tid * cs + (s_p - r0)];
+        if (col >= r0 && col < r1 && tid < jb) drow[par * NB + tid] = Ps[tid * cs + (col - r0)];
+        if (!grid_sync(pw.bar, G, phase, err)) return;
+        if (tid < 32) {
+            double bv = -1.0;
+            int bw = -1, brow = 0x7fffffff;
+            for (unsigned w = tid; w < G; w += 32) {
+                double v = __ldcg(pw.cand_val + par * G + w);
+                int ri = __ldcg(pw.cand_idx + par * G + w);
+                if (ri == 0x7fffffff) continue;
+                if (v > bv || (v == bv && ri < brow)) { bv = v; bw = (int)w; brow = ri; }
+            }
+            for (int o = 16; o; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                int ow = __shfl_xor_sync(0xffffffffu, bw, o), orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                if (ov > bv || (ov == bv && orow < brow)) { bv = ov; bw = ow; brow = orow; }
+            }
+            if (tid == 0) {
+                si[0] = bw;
+                s_p = brow;
+                if (b == 0 && bw >= 0) ipiv[col] = brow;
+            }
+        }
+        __syncthreads();
+        const int wb = si[0], p = s_p;
+        if (wb < 0) { dev_error(err, M25_DEV_INDEX); return; }
+        if (tid < jb) {
+            const volatile R *cu = (const volatile R *)(cand_row + ((size_t)par * G + wb) * NB + tid);
+            const volatile R *cd = (const volatile R *)(drow + par * NB + tid);
+            U[tid] = mk<R>(cu[0], cu[1]);
+            D[tid] = mk<R>(cd[0], cd[1]);
+        }
+        __syncthreads();
+        if (tid < jb) {
+            if (col >= r0 && col < r1) Ps[tid * cs + (col - r0)] = U[tid];
+            if (p != col && p >= r0 && p < r1) Ps[tid * cs + (p - r0)] = D[tid];
+        }
+        if (tid == 0) {
+            C piv = U[j];
+            if (piv.x == 0 && piv.y == 0) { dev_error(err, M25_DEV_ZEROPIV); s_recip = mk<R>(0, 0); }
+            else s_recip = cdiv<R>(mk<R>(1, 0), piv);
+        }
+        __syncthreads();
+        const C rc = s_recip;
+        const int i0 = max(0, col + 1 - r0), na = nr - i0;
+        for (int i = i0 + tid; i < nr; i += PANEL_THREADS) Ps[j * cs + i] = Ps[j * cs + i] * rc;
+        __syncthreads();
+        const int nc = jb - j - 1;
+        if (na > 0)
+            for (int e = tid; e < na * nc; e += PANEL_THREADS) {
+                int i = i0 + e % na, c = j + 1 + e / na;
+                C a = Ps[c * cs + i];
+                cfms<R>(a, Ps[j * cs + i], U[c]);
+                Ps[c * cs + i] = a;
+            }
+        __syncthreads();
+    }
+    for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
+        int c = e / nr, i = e % nr;
+        stc<R>(A, (size_t)(k0 + c) * lda + r0 + i, Ps[c * cs + i]);
+    }
+}
+
+// The same with the rows in global memory (when a block's rows do not fit in shared memory).
 template <typename R>
 __global__ void __launch_bounds__(PANEL_THREADS) k_panel(R *A, long lda, int n, int k0, int jb, int *ipiv, PanelWork pw,
                                                          int *err)
@@ -80,19 +197,27 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(R *A, long lda, int n, 
         if (col >= r0 && col < r1 && tid < jb) drow[par * NB + tid] = ldc<R>(A, (size_t)(k0 + tid) * lda + col);
         // 2. all blocks' candidates published
         if (!grid_sync(pw.bar, G, phase, err)) return;
-        // 3. the pivot: the best candidate over the blocks, the smallest row on ties
-        if (tid == 0) {
+        // 3. the pivot: the best candidate over the blocks, the smallest row on ties (one warp, loads in parallel,
+        //    past L1: the other blocks wrote them)
+        if (tid < 32) {
             double bv = -1.0;
             int bw = -1, brow = 0x7fffffff;
-            for (unsigned w = 0; w < G; ++w) {
-                double v = ((volatile double *)pw.cand_val)[par * G + w];
-                int ri = ((volatile int *)pw.cand_idx)[par * G + w];
+            for (unsigned w = tid; w < G; w += 32) {
+                double v = __ldcg(pw.cand_val + par * G + w);
+                int ri = __ldcg(pw.cand_idx + par * G + w);
                 if (ri == 0x7fffffff) continue;
                 if (v > bv || (v == bv && ri < brow)) { bv = v; bw = (int)w; brow = ri; }
             }
-            si[0] = bw;
-            s_p = brow;
-            if (b == 0) ipiv[col] = brow;
+            for (int o = 16; o; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                int ow = __shfl_xor_sync(0xffffffffu, bw, o), orow = __shfl_xor_sync(0xffffffffu, brow, o);
+                if (ov > bv || (ov == bv && orow < brow)) { bv = ov; bw = ow; brow = orow; }
+            }
+            if (tid == 0) {
+                si[0] = bw;
+                s_p = brow;
+                if (b == 0 && bw >= 0) ipiv[col] = brow;
+            }
         }
         __syncthreads();
         const int wb = si[0], p = s_p;
@@ -130,16 +255,15 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(R *A, long lda, int n, 
     }
 }
 
-// the panel's interchanges on the columns outside it: one thread per column, the swaps in order
+// interchanges ipiv[r0 .. r0 + nsw) applied in order to the columns [c0, c1): one thread per column
 template <typename R>
-__global__ void k_laswp(R *A, long lda, int n, int k0, int jb, const int *ipiv)
+__global__ void k_laswp(R *A, long lda, int n, int r0, int nsw, const int *ipiv, long c0, long c1)
 {
-    long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (c >= n - jb) return;
-    if (c >= k0) c += jb;                                  // skip the panel's own columns
+    long c = c0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (c >= c1) return;
     R *col = A + 2 * (size_t)c * lda;
-    for (int j = 0; j < jb; ++j) {
-        int p = ipiv[k0 + j], r = k0 + j;
+    for (int j = 0; j < nsw; ++j) {
+        int p = ipiv[r0 + j], r = r0 + j;
         if (p != r && p >= 0 && p < n) {
             cpx<R> a = ldc<R>(col, r), b = ldc<R>(col, p);
             stc<R>(col, r, b); stc<R>(col, p, a);
@@ -147,42 +271,50 @@ __global__ void k_laswp(R *A, long lda, int n, int k0, int jb, const int *ipiv)
     }
 }
 
-// U12 = L11^-1 A12: L11 (jb x jb, unit lower) in shared memory, each thread one column of A12
+// A[k0 .. k0 + jb, c0 .. c1) = L11^-1 A[k0 .. k0 + jb, c0 .. c1), L11 = A[k0 .., k0 ..] unit lower (jb <= NB), in
+// shared memory; each thread one column
+// 64 columns a block of 256 threads: column c = tid % 64, rows split 4 ways (k % 4 == tid / 64); after row i is final
+// the block updates the rows below it (one barrier a row)
 template <typename R>
-__global__ void __launch_bounds__(64) k_trsm(R *A, long lda, int n, int k0, int jb)
+__global__ void __launch_bounds__(256) k_trsm(R *A, long lda, int k0, int jb, long c0, long c1)
 {
     typedef cpx<R> C;
     extern __shared__ unsigned char sm_raw[];
-    C *L = reinterpret_cast<C *>(sm_raw);                  // L[i * NB + k]
-    C *X = L + NB * NB;                                    // X[i * 64 + thread]
+    C *L = reinterpret_cast<C *>(sm_raw);                  // L[k * NB + i] = L(k, i)
+    C *X = L + NB * NB;                                    // X[k * 64 + column]
     for (int e = threadIdx.x; e < jb * jb; e += blockDim.x) {
-        int k = e / jb, i = e % jb;                        // column k, row i (column-major read, coalesced)
-        L[i * NB + k] = ldc<R>(A, (size_t)(k0 + k) * lda + k0 + i);
+        int i = e / jb, k = e % jb;                        // column i, row k (coalesced)
+        L[k * NB + i] = ldc<R>(A, (size_t)(k0 + i) * lda + k0 + k);
     }
-    const long c = k0 + jb + blockIdx.x * (long)blockDim.x + threadIdx.x;
-    const bool live = c < n;
-    if (live)
-        for (int i = 0; i < jb; ++i) X[i * 64 + threadIdx.x] = ldc<R>(A, (size_t)c * lda + k0 + i);
+    const int cl = threadIdx.x & 63, g = threadIdx.x >> 6;
+    const long c = c0 + blockIdx.x * 64L + cl;
+    const bool live = c < c1;
+    for (int k = g; k < jb; k += 4) X[k * 64 + cl] = live ? ldc<R>(A, (size_t)c * lda + k0 + k) : mk<R>(0, 0);
     __syncthreads();
-    if (!live) return;
-    for (int i = 1; i < jb; ++i) {
-        C x = X[i * 64 + threadIdx.x];
-        for (int k = 0; k < i; ++k) cfms<R>(x, L[i * NB + k], X[k * 64 + threadIdx.x]);
-        X[i * 64 + threadIdx.x] = x;
+    for (int i = 0; i < jb - 1; ++i) {
+        const C xi = X[i * 64 + cl];
+        for (int k = i + 1 + ((g - (i + 1)) % 4 + 4) % 4; k < jb; k += 4) {
+            C x = X[k * 64 + cl];
+            cfms<R>(x, L[k * NB + i], xi);
+            X[k * 64 + cl] = x;
+        }
+        __syncthreads();
     }
-    for (int i = 0; i < jb; ++i) stc<R>(A, (size_t)c * lda + k0 + i, X[i * 64 + threadIdx.x]);
+    if (live)
+        for (int k = g; k < jb; k += 4) stc<R>(A, (size_t)c * lda + k0 + k, X[k * 64 + cl]);
 }
 
-// C (M x N) -= A (M x K) B (K x N), all column-major complex inside the factor (lda). 128 x 64 tile per block of
-// 256 threads, each 8 x 4 outputs; K staged 16 at a time through shared memory (the next slice prefetched into
-// registers while the current one is used).
+// C (M x N) -= A (M x K) B (K x N), all column-major complex inside the factor (lda). A 128 x 64 tile per block of
+// 256 threads, each 8 x 4 outputs; K staged BK at a time through two shared-memory buffers, the next slice loaded
+// into registers while the current one is multiplied (one barrier a slice).
 template <typename R>
 __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R *Bm, long lda, int M, int N, int K)
 {
     typedef cpx<R> C;
     constexpr int BM = 128, BN = 64, BK = 8;
-    __shared__ C As[BK][BM];
-    __shared__ C Bs[BK][BN + 1];
+    extern __shared__ unsigned char gemm_raw[];
+    C(*As)[BK][BM] = reinterpret_cast<C(*)[BK][BM]>(gemm_raw);                       // [2][BK][BM]
+    C(*Bs)[BK][BN + 1] = reinterpret_cast<C(*)[BK][BN + 1]>(gemm_raw + 2 * sizeof(C) * BK * BM);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     C acc[8][4];
@@ -190,31 +322,48 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
     for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = mk<R>(0, 0);
+    // each thread stages 4 A and 2 B elements a slice
+    C ra[4], rb[2];
+    auto load = [&](int kk) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int e = threadIdx.x + 256 * u, k = e / BM, m = e % BM;
+            ra[u] = (m0 + m < M && kk + k < K) ? ldc<R>(Am, (size_t)(kk + k) * lda + m0 + m) : mk<R>(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            int e = threadIdx.x + 256 * u, nn = e / BK, k = e % BK;
+            rb[u] = (n0 + nn < N && kk + k < K) ? ldc<R>(Bm, (size_t)(n0 + nn) * lda + kk + k) : mk<R>(0, 0);
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { int e = threadIdx.x + 256 * u; As[buf][e / BM][e % BM] = ra[u]; }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) { int e = threadIdx.x + 256 * u; Bs[buf][e % BK][e / BK] = rb[u]; }
+    };
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
     for (int kk = 0; kk < K; kk += BK) {
-        // A slice: BK columns of BM rows (coalesced along rows)
-        for (int e = threadIdx.x; e < BK * BM; e += 256) {
-            int k = e / BM, m = e % BM;
-            As[k][m] = (m0 + m < M && kk + k < K) ? ldc<R>(Am, (size_t)(kk + k) * lda + m0 + m) : mk<R>(0, 0);
-        }
-        // B slice: BN columns of BK rows (coalesced along k)
-        for (int e = threadIdx.x; e < BK * BN; e += 256) {
-            int nn = e / BK, k = e % BK;
-            Bs[k][nn] = (n0 + nn < N && kk + k < K) ? ldc<R>(Bm, (size_t)(n0 + nn) * lda + kk + k) : mk<R>(0, 0);
-        }
-        __syncthreads();
-#pragma unroll 4
+        const bool more = kk + BK < K;
+        if (more) load(kk + BK);
+#pragma unroll
         for (int k = 0; k < BK; ++k) {
             C a[8], b[4];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = As[k][ty + 16 * i];
+            for (int i = 0; i < 8; ++i) a[i] = As[buf][k][ty + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[buf][k][tx + 16 * j];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) cfma<R>(acc[i][j], a[i], b[j]);
         }
+        if (more) store(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -229,6 +378,9 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
         }
     }
 }
+
+template <typename R>
+static size_t gemm_smem() { return 2 * sizeof(cpx<R>) * 8 * 128 + 2 * sizeof(cpx<R>) * 8 * 65; }
 
 // ---- triangular solves with the factor of A = Z^T: Z X = B (zgetrs, trans = 'T') -------------------------------------
 // U^T y = b (forward, non-unit), L^T z = y (backward, unit), X = P z. B row-major n x nrhs. Blocks of TB rows: the
@@ -369,33 +521,74 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     M25_CHECK(cudaMemsetAsync(ipiv, 0xff, sizeof(int) * (size_t)n, s));      // -1 until the panel sets it
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
     M25_CHECK(cudaFuncSetAttribute(k_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
-    for (int k0 = 0; k0 < n; k0 += NB) {
-        const int jb = std::min(NB, n - k0);
-        int Gp = std::min(G, std::max(1, (n - k0 + 63) / 64));
-        M25_CHECK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
-        void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
-        M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, s));
-        if (n - jb > 0) {
-            long cols = n - jb;
-            k_laswp<R><<<(cols + 127) / 128, 128, 0, s>>>(A, lda, n, k0, jb, ipiv);
-            M25_LAUNCH_CHECK("k_laswp");
+    int smem_optin = 0, dev = 0;
+    M25_CHECK(cudaGetDevice(&dev));
+    M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int smem_cap = smem_optin - 4096;                          // (the kernel's static shared memory)
+    M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+    int gmax = G;                                                    // blocks of the panel (M25_PANEL_BLOCKS: tuning)
+    if (const char *e = getenv("M25_PANEL_BLOCKS")) gmax = std::max(1, std::min(G, atoi(e)));
+    int nb2 = NB2;                                                   // outer panel (M25_NB2: tuning, a multiple of NB)
+    if (const char *e = getenv("M25_NB2")) nb2 = std::max(NB, atoi(e) / NB * NB);
+    M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
+    auto laswp = [&](int r0, int nsw, long c0, long c1) -> int {
+        if (c1 <= c0) return M25_OK;
+        k_laswp<R><<<(c1 - c0 + 127) / 128, 128, 0, s>>>(A, lda, n, r0, nsw, ipiv, c0, c1);
+        M25_LAUNCH_CHECK("k_laswp");
+        return M25_OK;
+    };
+    auto trsm = [&](int k0, int jb, long c0, long c1) -> int {
+        if (c1 <= c0) return M25_OK;
+        k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, s>>>(A, lda, k0, jb, c0, c1);
+        M25_LAUNCH_CHECK("k_trsm");
+        return M25_OK;
+    };
+    // C = A[r0 .., c0 ..] (M x Nc) -= A[r0 .., k0 .. k0 + K] A[k0 .. k0 + K, c0 ..]
+    auto gemm = [&](int r0, int M, long c0, int Nc, int k0, int K, bool big) -> int {
+        if (M <= 0 || Nc <= 0 || K <= 0) return M25_OK;
+        R *C22 = A + 2 * ((size_t)c0 * lda + r0);
+        const R *L21 = A + 2 * ((size_t)k0 * lda + r0);
+        const R *U12 = A + 2 * ((size_t)c0 * lda + k0);
+        if (sizeof(R) == 4 && tf32 && big)
+            return m25_umma_trailing((float *)C22, lda, M, Nc, K, (const float *)L21, (const float *)U12, umma_work,
+                                     umma_bytes, s);
+        dim3 grid((Nc + 63) / 64, (M + 127) / 128);
+        k_gemm_update<R><<<grid, 256, gemm_smem<R>(), s>>>(C22, L21, U12, lda, M, Nc, K);
+        M25_LAUNCH_CHECK("k_gemm_update");
+        return M25_OK;
+    };
+    int rc;
+    // Two levels: outer panels of nb2 columns, each factored as panels of NB (pivoting, interchanges, TRSM and
+    // updates restricted to the outer panel); then the outer panel's interchanges, TRSM and one trailing update
+    // of depth nb2 over the rest of the matrix.
+    for (int K0 = 0; K0 < n; K0 += nb2) {
+        const int JB = std::min(nb2, n - K0), KE = K0 + JB;
+        for (int k0 = K0; k0 < KE; k0 += NB) {
+            const int jb = std::min(NB, KE - k0);
+            int Gp = std::min(gmax, std::max(1, (n - k0 + 31) / 32));
+            const int cs = (n - k0 + Gp - 1) / Gp;
+            const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
+            M25_CHECK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+            void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
+            if (psmem <= (size_t)smem_cap)
+                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R>, dim3(Gp), dim3(PANEL_THREADS), args,
+                                                      psmem, s));
+            else
+                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, s));
+            m25_note_launch();
+            if ((rc = laswp(k0, jb, 0, k0))) return rc;                    // left: the factored L columns
+            if ((rc = laswp(k0, jb, k0 + jb, KE))) return rc;              // the rest of the outer panel
+            if ((rc = trsm(k0, jb, k0 + jb, KE))) return rc;
+            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, false))) return rc;
         }
-        const int rest = n - k0 - jb;
-        if (rest > 0) {
-            k_trsm<R><<<(rest + 63) / 64, 64, trsm_smem, s>>>(A, lda, n, k0, jb);
-            M25_LAUNCH_CHECK("k_trsm");
-            R *C22 = A + 2 * ((size_t)(k0 + jb) * lda + k0 + jb);
-            const R *L21 = A + 2 * ((size_t)k0 * lda + k0 + jb);
-            const R *U12 = A + 2 * ((size_t)(k0 + jb) * lda + k0);
-            if (sizeof(R) == 4 && tf32) {
-                int rc = m25_umma_trailing((float *)C22, lda, rest, rest, jb, (const float *)L21, (const float *)U12,
-                                           umma_work, umma_bytes, s);
-                if (rc) return rc;
-            } else {
-                dim3 grid((rest + 63) / 64, (rest + 127) / 128);
-                k_gemm_update<R><<<grid, 256, 0, s>>>(C22, L21, U12, lda, rest, rest, jb);
-                M25_LAUNCH_CHECK("k_gemm_update");
+        if (KE < n) {
+            if ((rc = laswp(K0, JB, KE, n))) return rc;                    // the outer panel's interchanges, right
+            for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
+                const int jb = std::min(NB, KE - k0);
+                if ((rc = trsm(k0, jb, KE, n))) return rc;
+                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, false))) return rc;
             }
+            if ((rc = gemm(KE, n - KE, KE, n - KE, K0, JB, true))) return rc;   // the trailing update, depth nb2
         }
     }
     return M25_OK;

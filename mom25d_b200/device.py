@@ -17,7 +17,9 @@ from .board import MU0, C0, EPS0
 
 c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
 
-TABLE_NRHO, TABLE_NFINE, TABLE_NFINE32 = 260, 8192, 4096      # multilayer.py:260 defaults; the mixed fill's tables
+# multilayer.py:260 defaults; the mixed fill's complex64 tables keep the same grid (at 4096 points their linear
+# interpolation differed from the double tables by ~1e-3 near rho = 0: too weak a preconditioner at low frequency)
+TABLE_NRHO, TABLE_NFINE, TABLE_NFINE32 = 260, 8192, 8192
 VIA_NRHO = 200                                                # via.py:179
 VIA_TABLE_PAIRS = 64                                          # sim.py:784
 

@@ -152,10 +152,15 @@ class DirectSolver:
         N = self.geo.N
         ipiv = self._buf('ipiv', (N,), torch.int32)
         work = self._getrf_work(N, single)
+        st = self.stream if self.stream is not None else torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
         check(lib().m25_getrf(P(Z), c_long(N), c_int(N), P(ipiv), c_int(int(single)),
                               c_int(int(single and self.tf32)), P(work), ctypes.c_size_t(work.numel()), self.s),
               'm25_getrf')
+        b.record(st)
         _lib.sync_check(self.stream, 'm25_getrf')
+        self.last_lu_ms = a.elapsed_time(b)                # the factorisation alone, on its stream
         return ipiv
 
     def _lu_solve(self, Z, ipiv, R, single):

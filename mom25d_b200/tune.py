@@ -1,0 +1,68 @@
+"""
+mom25d_b200.tune - timings of the hot path's kernels on this GPU, and the choice of their tile parameters.
+
+    python -m mom25d_b200.tune --lu 8192 [--single] [--tf32] [--reps 3]     # the LU alone, CUDA events
+    python -m mom25d_b200.tune --fill                                        # fill / near / tables, 20k board
+
+Times are CUDA-event measurements on the launching stream after a warm-up, the matrix a random complex one with a
+dominant diagonal (pivots away from it as well).
+"""
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import P, check, lib
+
+
+def random_matrix(n, dtype, seed=0):
+    g = torch.Generator(device='cuda').manual_seed(seed)
+    rdt = torch.float32 if dtype == torch.complex64 else torch.float64
+    Z = torch.complex(torch.randn(n, n, generator=g, device='cuda', dtype=rdt),
+                      torch.randn(n, n, generator=g, device='cuda', dtype=rdt))
+    Z.diagonal().add_(4 * n ** 0.5)
+    return Z
+
+
+def time_lu(n, single=False, tf32=False, reps=3):
+    dtype = torch.complex64 if single else torch.complex128
+    Z0 = random_matrix(n, dtype)
+    Z = torch.empty_like(Z0)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(lib().m25_getrf_workspace(n, int(single)))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    out = []
+    for r in range(reps + 1):
+        Z.copy_(Z0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s = torch.cuda.current_stream()
+        a.record(s)
+        check(lib().m25_getrf(P(Z), ctypes.c_long(n), n, P(ipiv), int(single), int(tf32), P(work), ctypes.c_size_t(nb),
+                              _lib.stream_ptr()), 'm25_getrf')
+        b.record(s)
+        _lib.sync_check()
+        if r:
+            out.append(a.elapsed_time(b))
+    ms = float(np.median(out))
+    flops = 8.0 / 3.0 * n ** 3
+    return dict(n=n, single=single, tf32=tf32, ms=ms, tflops=flops / ms / 1e9)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--lu', type=int, default=0)
+    ap.add_argument('--single', action='store_true')
+    ap.add_argument('--tf32', action='store_true')
+    ap.add_argument('--reps', type=int, default=3)
+    a = ap.parse_args()
+    _lib.require_cuda()
+    if a.lu:
+        print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
+
+
+if __name__ == '__main__':
+    main()

@@ -75,10 +75,10 @@ def test_green_tables_match(small, f):
     for k in ('cAi', 'cqi'):
         assert np.allclose(hd[k], od.tb[k], rtol=1e-6, atol=0), k
     assert np.array_equal(hd['kind'], od.tb['kind'])
-    # the mixed fill's complex64 tables: the same spline on 4096 points, rounded
+    # the mixed fill's complex64 tables: the same spline on the same grid, rounded
     A32 = dt.AQ32.cpu().numpy()
     n = len(hd['kind'])
-    rho32 = np.linspace(0, geo.rho_max, 4096)
+    rho32 = np.linspace(0, geo.rho_max, A32.shape[1])
     from scipy.interpolate import CubicSpline
     H = dt.H.cpu().numpy()
     for i in range(n):
@@ -209,3 +209,34 @@ def test_complex_bessel_matches_the_reference(golden):
                                                     _lib.stream_ptr()))
         ref = golden['jn_%d' % n]
         assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize('n', [700, 2000])
+def test_lu_with_tensor_core_updates(n):
+    """The complex64 LU with its trailing updates on the tensor cores (3xTF32): a factor as good as the FP32 one
+    (backward error at single-precision level) and solves that match."""
+    from mom25d_b200 import _lib
+    rng = np.random.default_rng(5)
+    Z = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    Z += (4 * np.sqrt(n) * np.eye(n)).astype(np.complex64)
+    Zd = _lib.dev(Z)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(_lib.lib().m25_getrf_workspace(n, 1))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    _lib.check(_lib.lib().m25_getrf(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), 1, 1, _lib.P(work),
+                                    ctypes.c_size_t(nb), _lib.stream_ptr()))
+    _lib.sync_check()
+    lu_ref, piv_ref = sla.lu_factor(Z.T.astype(complex))
+    lu = Zd.cpu().numpy().T
+    assert np.mean(ipiv.cpu().numpy() == piv_ref) > 0.99        # (rounding may move a near-tie)
+    P = np.arange(n)
+    for i, p in enumerate(ipiv.cpu().numpy()):
+        P[[i, p]] = P[[p, i]]
+    Lm, Um = np.tril(lu, -1) + np.eye(n), np.triu(lu)
+    A = Z.T.astype(complex)
+    assert np.abs(Lm @ Um - A[P]).max() < 1e-5 * np.abs(A).max()
+    R = rng.standard_normal((n, 2)) + 1j * rng.standard_normal((n, 2))
+    x = np.linalg.solve(Z.astype(complex), R)
+    Rd = _lib.dev(R.astype(np.complex64))
+    _lib.check(_lib.lib().m25_getrs(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), 1, _lib.P(Rd), 2, _lib.stream_ptr()))
+    assert np.abs(Rd.cpu().numpy() - x).max() < 1e-4 * np.abs(x).max()
