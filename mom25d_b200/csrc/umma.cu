@@ -21,8 +21,12 @@ int *m25_dev_err_word();
 
 namespace {
 
-constexpr int BM = 128, BN = 256, BKF = 32;          // tile of C' (rows x cols), K floats per stage
-constexpr int STAGES = 2;
+// tile of C' (rows x cols), K floats per stage (16 floats = 64 B rows: 64B swizzle), stages in the ring: three
+// stages in flight while one is multiplied
+constexpr int BM = 128, BN = 256, BKF = 16;
+constexpr int STAGES = 4;
+constexpr int SWZ_BYTES = BKF * 4;                   // the swizzle span: one K row of a stage
+static_assert(SWZ_BYTES == 64 || SWZ_BYTES == 128, "64B or 128B swizzle");
 constexpr int A_BYTES = BM * BKF * 4, B_BYTES = BN * BKF * 4;
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;          // hi and lo of A' and B'
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // + alignment slack + barriers
@@ -63,15 +67,16 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
                  ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar) : "memory");
 }
 
-// shared-memory matrix descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart (tcgen05 layout, version 1)
+// shared-memory matrix descriptor: K-major, swizzled rows of SWZ_BYTES, 8-row groups 8 x SWZ_BYTES apart
+// (tcgen05 layout, version 1; layout type 2 = 128B swizzle, 4 = 64B swizzle)
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr)
 {
     uint64_t d = 0;
     d |= (uint64_t)((addr & 0x3FFFF) >> 4);
     d |= (uint64_t)(16 >> 4) << 16;          // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset
+    d |= (uint64_t)((8 * SWZ_BYTES) >> 4) << 32;   // stride byte offset
     d |= (uint64_t)1 << 46;                  // descriptor version
-    d |= (uint64_t)2 << 61;                  // SWIZZLE_128B
+    d |= (uint64_t)(SWZ_BYTES == 128 ? 2 : 4) << 61;
     return d;
 }
 
@@ -192,14 +197,16 @@ __global__ void __launch_bounds__(128, 1) k_umma_update(float *C, long ldc_f, in
                          : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row < Mp) {
+                // all 32 loads issued before any store (a load -> store chain per column serialised the memory
+                // latency 256 times a tile)
+                float cv[32];
+                float *p = C + (size_t)(n0 + c0) * ldc_f + row;
+                const int nv = min(32, Nc - (n0 + c0));
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int n = n0 + c0 + j;
-                    if (n < Nc) {
-                        float *p = C + (size_t)n * ldc_f + row;
-                        *p = *p - __uint_as_float(v[j]);
-                    }
-                }
+                for (int j = 0; j < 32; ++j) cv[j] = j < nv ? __ldcg(p + (size_t)j * ldc_f) : 0.f;
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (j < nv) __stcg(p + (size_t)j * ldc_f, cv[j] - __uint_as_float(v[j]));
             }
         }
     }
@@ -284,7 +291,9 @@ int make_map(CUtensorMap *m, const float *ptr, long rows, long cols, long pitch_
     cuuint32_t box[2] = {(cuuint32_t)BKF, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)ptr, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     SWZ_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) { m25_set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return M25_ECUDA; }
     return M25_OK;

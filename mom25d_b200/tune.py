@@ -52,8 +52,34 @@ def time_lu(n, single=False, tf32=False, reps=3):
     return dict(n=n, single=single, tf32=tf32, ms=ms, tflops=flops / ms / 1e9)
 
 
+def time_update(M, N, K, reps=5):
+    """The complex64 trailing update C -= L U alone: tensor cores (3xTF32) and, for comparison, the LU's SIMT
+    kernel through a factorisation-free call are both timed with CUDA events. 8 M N K flops."""
+    ld = max(M, K)
+    C = random_matrix(max(ld, N), torch.complex64)[:N, :].contiguous()          # N columns of ld
+    L = random_matrix(max(ld, K), torch.complex64, seed=1)[:K, :].contiguous()
+    U = random_matrix(max(ld, N), torch.complex64, seed=2)[:N, :].contiguous()
+    nb = int((2 * 2 * M * 512 + 2 * N * 512) * 4 + 4096)
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    s = torch.cuda.current_stream()
+    out = []
+    for r in range(reps + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        check(lib().m25_cgemm_update_tf32(P(C), ctypes.c_long(C.shape[1]), M, N, K, P(L), P(U), P(work),
+                                          ctypes.c_size_t(nb), _lib.stream_ptr()), 'm25_cgemm_update_tf32')
+        b.record(s)
+        _lib.sync_check()
+        if r:
+            out.append(a.elapsed_time(b))
+    ms = float(np.median(out))
+    return dict(M=M, N=N, K=K, ms=ms, tflops_complex=8.0 * M * N * K / ms / 1e9,
+                tflops_tf32_issued=3 * 8.0 * M * N * K / ms / 1e9)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument('--update', type=int, nargs=3, default=None, metavar=('M', 'N', 'K'))
     ap.add_argument('--lu', type=int, default=0)
     ap.add_argument('--single', action='store_true')
     ap.add_argument('--tf32', action='store_true')
@@ -62,6 +88,8 @@ def main():
     _lib.require_cuda()
     if a.lu:
         print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
+    if a.update:
+        print(json.dumps(time_update(*a.update, reps=a.reps)))
 
 
 if __name__ == '__main__':
