@@ -148,7 +148,10 @@ def run_gpu(args, rank, world):
     sim = Simulation.from_board(bd, precision='mixed')
     geo = sim.geo
     ds = sim.fast
-    mine = [f for i, f in enumerate(FREQS) if i % world == rank]
+    # the sweep's frequencies in a strided order (step i: FREQS[8 i mod 21]), so a run of fewer than 21 steps
+    # samples the whole band rather than its low end; ranks take every world-th
+    order = [FREQS[(8 * i) % len(FREQS)] for i in range(len(FREQS))]
+    mine = [f for i, f in enumerate(order) if i % world == rank]
     E_host = torch.from_numpy(geo.excitation()).pin_memory()
     E_dev = E_host.to('cuda')
     stream = torch.cuda.current_stream()
@@ -187,6 +190,7 @@ def run_gpu(args, rank, world):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     lat, lu_ms, iters = [], [], []
+    ds.timings = {}
     for i in range(args.steps):
         ms, lms = step_device(mine[i % len(mine)], 'mixed')
         lat.append(ms); lu_ms.append(lms); iters.append(max(ds.iters) if ds.iters else 0)
@@ -195,6 +199,7 @@ def run_gpu(args, rank, world):
     clocks = clk.stop()
     launches = lib.m25_launch_count() - n0
     t_dev = ev0.elapsed_time(ev1) / 1000.0
+    phases = {k: round(1000 * v / args.steps, 2) for k, v in ds.timings.items()}
     # FP64 drop-in path
     lat64, lu64 = [], []
     for i in range(args.fp64_steps):
@@ -246,7 +251,7 @@ def run_gpu(args, rank, world):
                  "lu_ms": round(statistics.mean(lu64), 3) if lu64 else None},
         "mixed_over_fp64": round(value / fp64, 3) if fp64 else None,
         "max_dS_mixed_vs_fp64": dS, "mixed_rel_residual": res_m, "gmres_iters_max": int(max(iters)),
-        "lu_ms": round(1000 * lu_avg, 3),
+        "lu_ms": round(1000 * lu_avg, 3), "phases_ms_per_step": phases,
         "e2e": {"value": round(e2e, 4), "unit": "freq-solves/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},
         "gpu_launches": int(launches),
@@ -287,7 +292,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--steps', type=int, default=21)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--fp64-steps', type=int, default=3)
     ap.add_argument('--impl', default='b200')

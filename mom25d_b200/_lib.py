@@ -52,6 +52,7 @@ def lib():
         L.m25_version.restype = ctypes.c_char_p
         L.m25_last_error.restype = ctypes.c_char_p
         L.m25_getrf_workspace.restype = ctypes.c_size_t
+        L.m25_getrs_aux_bytes.restype = ctypes.c_size_t
         L.m25_getrf_workspace.argtypes = [ctypes.c_int, ctypes.c_int]
         L.m25_pair_record_bytes.restype = ctypes.c_size_t
         _lib = L

@@ -411,23 +411,26 @@ __global__ void __launch_bounds__(128) k_mv_pairs(int K, m25_mesh g, m25_tables 
     const int lp = live ? g.lt[p] : 0;
     zd ax[KMAX], ay[KMAX], aq[KMAX];
     for (int c = 0; c < KMAX; ++c) ax[c] = ay[c] = aq[c] = mk<double>(0, 0);
-    for (int q0 = 0; q0 < g.Nt; q0 += QT) {
+    // this block's chunk of source triangles (grid.y chunks; partial sums added atomically)
+    const int chunk = (g.Nt + gridDim.y - 1) / gridDim.y;
+    const int qb = blockIdx.y * chunk, qe = min(g.Nt, qb + chunk);
+    for (int q0 = qb; q0 < qe; q0 += QT) {
         __syncthreads();
         for (int j = threadIdx.x; j < QT; j += 128) {
             int q = q0 + j;
-            sc[j][0] = q < g.Nt ? g.cent[2 * q] : 0; sc[j][1] = q < g.Nt ? g.cent[2 * q + 1] : 0;
-            sl[j] = q < g.Nt ? g.lt[q] : 0;
+            sc[j][0] = q < qe ? g.cent[2 * q] : 0; sc[j][1] = q < qe ? g.cent[2 * q + 1] : 0;
+            sl[j] = q < qe ? g.lt[q] : 0;
         }
         for (int j = threadIdx.x; j < QT * K; j += 128) {
             int qq = j / K, c = j % K, q = q0 + qq;
             zd z0 = mk<double>(0, 0);
-            S0[qq][c] = q < g.Nt ? ldc<double>(s0, (size_t)q * K + c) : z0;
-            SX[qq][c] = q < g.Nt ? ldc<double>(s1x, (size_t)q * K + c) : z0;
-            SY[qq][c] = q < g.Nt ? ldc<double>(s1y, (size_t)q * K + c) : z0;
+            S0[qq][c] = q < qe ? ldc<double>(s0, (size_t)q * K + c) : z0;
+            SX[qq][c] = q < qe ? ldc<double>(s1x, (size_t)q * K + c) : z0;
+            SY[qq][c] = q < qe ? ldc<double>(s1y, (size_t)q * K + c) : z0;
         }
         __syncthreads();
         if (!live) continue;
-        int qn = min(QT, g.Nt - q0);
+        int qn = min(QT, qe - q0);
         for (int j = 0; j < qn; ++j) {
             double dx = cx - sc[j][0], dy = cy - sc[j][1];
             zd ga, gq;
@@ -440,8 +443,10 @@ __global__ void __launch_bounds__(128) k_mv_pairs(int K, m25_mesh g, m25_tables 
     }
     if (!live) return;
     for (int c = 0; c < K; ++c) {
-        stc<double>(vAx, (size_t)p * K + c, ax[c]); stc<double>(vAy, (size_t)p * K + c, ay[c]);
-        stc<double>(wQ, (size_t)p * K + c, aq[c]);
+        size_t o = 2 * ((size_t)p * K + c);
+        atomicAdd(vAx + o, ax[c].x); atomicAdd(vAx + o + 1, ax[c].y);
+        atomicAdd(vAy + o, ay[c].x); atomicAdd(vAy + o + 1, ay[c].y);
+        atomicAdd(wQ + o, aq[c].x); atomicAdd(wQ + o + 1, aq[c].y);
     }
 }
 
@@ -613,7 +618,11 @@ extern "C" int m25_matvec_far_multi(const double *d_X, int K, double *d_Y, doubl
     long tot = (long)g->Nt * K;
     k_mv_aggregate<<<(tot + 255) / 256, 256, 0, S(stream)>>>(d_X, K, *g, s0, s1x, s1y);
     M25_LAUNCH_CHECK("k_mv_aggregate");
-    int blocks = (g->Nt + 127) / 128;
+    M25_CHECK(cudaMemsetAsync(vAx, 0, 3 * nk * sizeof(double), S(stream)));     // vAx, vAy, wQ: atomic sums
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    dim3 blocks((g->Nt + 127) / 128, 1);
+    blocks.y = std::max(1, std::min(64, (4 * sms + (int)blocks.x - 1) / (int)blocks.x));   // ~4 blocks an SM
     if (K <= 4)
         k_mv_pairs<4><<<blocks, 128, 0, S(stream)>>>(K, *g, *tb, s0, s1x, s1y, vAx, vAy, wQ);
     else if (K <= 8)

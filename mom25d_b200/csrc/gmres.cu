@@ -85,6 +85,46 @@ __global__ void k_coo_spmm(const int *ri, const int *ci, const double *vv, long 
     }
 }
 
+// Y[e, c] += sum over the near field's triplets of row e of vv X[col, c], one warp per edge e. Row e's triplets are
+// the slots 9 i + 3 s + u of the pairs i whose observation triangle is one of e's two triangles (the pairs are sorted
+// by it: off[t] .. off[t + 1]), s the slot of e on that triangle; the column is te[3 Q[i] + u]. A fixed order:
+// deterministic sums, no atomics.
+__global__ void k_near_rows_spmm(m25_mesh g, const long long *off, const int *Q, const double *vv, const double *X,
+                                 int k, double *Y)
+{
+    const int e = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32, lane = threadIdx.x & 31;
+    if (e >= g.Ne) return;
+    double ax[16], ay[16];
+    for (int c = 0; c < 16; ++c) ax[c] = ay[c] = 0;
+    for (int h = 0; h < 2; ++h) {
+        const int t = h ? g.em[e] : g.ep[e];
+        int s = 0;
+        while (s < 3 && g.te[3 * t + s] != e) ++s;
+        if (s == 3) continue;
+        const long long i0 = off[t], i1 = off[t + 1];
+        for (long long j = i0 * 3 + lane; j < i1 * 3; j += 32) {
+            const long long i = j / 3;
+            const int u = (int)(j % 3);
+            const int col = g.te[3 * Q[i] + u];
+            if (col < 0) continue;
+            const zd v = ldc<double>(vv, (size_t)(9 * i + 3 * s + u));
+            for (int c = 0; c < k; ++c) {
+                const zd x = ldc<double>(X, (size_t)col * k + c);
+                ax[c] = fma(v.x, x.x, ax[c]); ax[c] = fma(-v.y, x.y, ax[c]);
+                ay[c] = fma(v.x, x.y, ay[c]); ay[c] = fma(v.y, x.x, ay[c]);
+            }
+        }
+    }
+    for (int c = 0; c < k; ++c) {
+        double x = ax[c], y = ay[c];
+        for (int o = 16; o; o >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, o); y += __shfl_xor_sync(0xffffffffu, y, o); }
+        if (lane == 0) {
+            zd cur = ldc<double>(Y, (size_t)e * k + c);
+            stc<double>(Y, (size_t)e * k + c, cur + mk<double>(x, y));
+        }
+    }
+}
+
 // Z (complex64, ld) += vv at (ri, ci) (the near field into the mixed-precision matrix)
 __global__ void k_coo_add_c64(const int *ri, const int *ci, const double *vv, long nnz, float *Z, long ld)
 {
@@ -172,6 +212,16 @@ extern "C" int m25_coo_spmm(const int *d_ri, const int *d_ci, const double *d_vv
     if (!nnz) return M25_OK;
     k_coo_spmm<<<(nnz + 255) / 256, 256, 0, S(stream)>>>(d_ri, d_ci, d_vv, nnz, d_X, k, d_Y);
     M25_LAUNCH_CHECK("k_coo_spmm");
+    return M25_OK;
+}
+
+extern "C" int m25_near_spmm_rows(const m25_mesh *g, const long long *d_off, const int *d_Q, const double *d_vv,
+                                  const double *d_X, int k, double *d_Y, void *stream)
+{
+    M25_REQUIRE(g && k >= 1 && k <= 16, "m25_near_spmm_rows: mesh, 1 to 16 columns");
+    if (!g->Ne) return M25_OK;
+    k_near_rows_spmm<<<(g->Ne + 7) / 8, 256, 0, S(stream)>>>(*g, d_off, d_Q, d_vv, d_X, k, d_Y);
+    M25_LAUNCH_CHECK("k_near_rows_spmm");
     return M25_OK;
 }
 

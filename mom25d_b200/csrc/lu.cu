@@ -447,6 +447,180 @@ __global__ void __launch_bounds__(256) k_tri_update(const R *A, long lda, int i0
     }
 }
 
+// ---- solves with diagonal-block inverses (the reference's GPU solve design, gpu_vk.py:242-290) -----------------------
+// Once per factorisation (k_block_inverses): for every diagonal block of TB rows, inv(L_bb) (unit lower) and
+// inv(U_bb) (upper), one CTA a block, thread j forming column j of each. Per solve (k_trsv_step): one launch per
+// block; every CTA applies the block's inverse (transposed) to the block's running right-hand sides, CTA 0 stores
+// the result, and all CTAs update the right-hand sides of the unknowns still to come (a contiguous factor segment
+// per unknown, a warp per unknown).
+template <typename R>
+__global__ void __launch_bounds__(TB) k_block_inverses(const R *A, long lda, int n, R *inv)
+{
+    typedef cpx<R> C;
+    extern __shared__ unsigned char inv_raw[];
+    C(*D)[TB + 1] = reinterpret_cast<C(*)[TB + 1]>(inv_raw);          // D[r][c] = A[b0 + r, b0 + c]
+    C(*X)[TB + 1] = reinterpret_cast<C(*)[TB + 1]>(inv_raw + sizeof(C) * TB * (TB + 1));   // column j: thread j
+    const int b = blockIdx.x, b0 = b * TB, bs = min(TB, n - b0), j = threadIdx.x;
+    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+        int c = e / TB, r = e % TB;                         // identity outside the block's bs x bs corner
+        D[r][c] = (r < bs && c < bs) ? ldc<R>(A, (size_t)(b0 + c) * lda + b0 + r) : mk<R>(r == c ? 1 : 0, 0);
+    }
+    __syncthreads();
+    R *iL = inv + 2 * ((size_t)b * 2 * TB * TB), *iU = iL + 2 * (size_t)TB * TB;     // [r][c] row-major
+    // column j of inv(L), L unit lower: x_i = delta_ij - sum_{j <= k < i} L[i][k] x_k
+    for (int i = 0; i < TB; ++i) {
+        C v = mk<R>(i == j ? 1 : 0, 0);
+        for (int k = j; k < i; ++k) cfms<R>(v, D[i][k], X[k][j]);
+        X[i][j] = i < j ? mk<R>(0, 0) : v;
+    }
+    for (int i = 0; i < TB; ++i) stc<R>(iL, (size_t)i * TB + j, X[i][j]);
+    // column j of inv(U): x_j = 1 / U[j][j]; x_i = -(sum_{i < k <= j} U[i][k] x_k) / U[i][i], i = j-1 .. 0
+    for (int i = TB - 1; i >= 0; --i) {
+        C v = mk<R>(0, 0);
+        if (i == j) v = cdiv<R>(mk<R>(1, 0), D[j][j]);
+        else if (i < j) {
+            for (int k = i + 1; k <= j; ++k) cfma<R>(v, D[i][k], X[k][j]);
+            v = cdiv<R>(mk<R>(-v.x, -v.y), D[i][i]);
+        }
+        X[i][j] = v;
+    }
+    for (int i = 0; i < TB; ++i) stc<R>(iU, (size_t)i * TB + j, X[i][j]);
+}
+
+// The whole triangular solve in one cooperative launch, no kernel boundary between blocks. CTA g owns the row blocks
+// [bb0, bb1) (contiguous) and keeps their running right-hand sides in shared memory. Blocks are visited in solve
+// order (forward: 0 .. nb-1 for U^T; backward: nb-1 .. 0 for L^T):
+//   a block of another CTA that precedes mine: wait for its flag (bounded), read its solved values, apply them to
+//     my rows (the factor's column segment of each of my rows: contiguous);
+//   a block of mine: every earlier block has been applied to it, so solve it with its inverse (transposed),
+//     publish the values (store, fence, flag = epoch), then apply them to my other rows still to come.
+// The flags only point backwards in solve order and all CTAs are co-resident: no cycle, every wait ends.
+template <typename R>
+struct TrsvArgs {
+    const R *A; long lda; int n; int nb;
+    const R *inv;          // block inverses: per block, inv(L_bb) then inv(U_bb), TB x TB row-major each
+    const R *Tin;          // right-hand sides (n x nrhs)
+    R *Xout;               // solution (n x nrhs)
+    int nrhs; int backward;
+    int *flags; const int *epoch_ptr; int *err;   // flags[b] == *epoch_ptr: block b solved in this call
+};
+
+__global__ void k_bump_epoch(int *e) { *e += 1; }
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_trsv_persistent(TrsvArgs<R> a)
+{
+    typedef cpx<R> C;
+    extern __shared__ unsigned char tp_raw[];
+    const int G = gridDim.x, g = blockIdx.x, nb = a.nb, nrhs = a.nrhs;
+    const int epoch = *(volatile const int *)a.epoch_ptr;
+    const int per = (nb + G - 1) / G, bb0 = g * per, bb1 = min(nb, bb0 + per);
+    const int R0 = bb0 * TB, R1 = min(a.n, bb1 * TB), nr = max(0, R1 - R0);
+    C(*Ws)[TB + 1] = reinterpret_cast<C(*)[TB + 1]>(tp_raw);
+    C(*Yb)[16] = reinterpret_cast<C(*)[16]>(tp_raw + sizeof(C) * TB * (TB + 1));
+    C(*T)[16] = reinterpret_cast<C(*)[16]>(tp_raw + sizeof(C) * (TB * (TB + 1) + TB * 16));
+    __shared__ int ok;
+    for (int e = threadIdx.x; e < nr * nrhs; e += blockDim.x)
+        T[e / nrhs][e % nrhs] = ldc<R>(a.Tin, (size_t)(R0 + e / nrhs) * nrhs + e % nrhs);
+    if (threadIdx.x == 0) ok = 1;
+    __syncthreads();
+    if (nr == 0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // one lane a row: lane l of warp w takes row ra + 32 w + l (+ 256 per round) and streams its factor segment
+    // A[b0 .. b0 + bs, r] (contiguous) against Yb (a shared-memory broadcast); no reductions across lanes
+    auto prefetch = [&](int b0, int bs, int ra, int rb) {          // the segments into L1 while the flag is awaited
+        for (int r = ra + threadIdx.x; r < rb; r += blockDim.x) {
+            const char *p = reinterpret_cast<const char *>(a.A + 2 * ((size_t)r * a.lda + b0));
+            for (int off = 0; off < bs * (int)sizeof(C); off += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + off));
+        }
+    };
+    auto apply = [&](int b0, int bs, int ra, int rb, bool) {
+        for (int r = ra + threadIdx.x; r < rb; r += blockDim.x) {
+            const C *seg = reinterpret_cast<const C *>(a.A) + (size_t)r * a.lda + b0;
+            C acc[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) acc[c] = mk<R>(0, 0);
+#pragma unroll 4
+            for (int k = 0; k < bs; ++k) {
+                const C v = seg[k];
+#pragma unroll
+                for (int c = 0; c < 16; ++c)
+                    if (c < nrhs) cfma<R>(acc[c], v, Yb[k][c]);
+            }
+#pragma unroll
+            for (int c = 0; c < 16; ++c)
+                if (c < nrhs) T[r - R0][c] -= acc[c];
+        }
+    };
+    bool ws_ready = false;
+    {                                                               // my first block's inverse, ahead of time
+        const int first = a.backward ? bb1 - 1 : bb0;
+        const int fs = min(TB, a.n - first * TB);
+        const R *W = a.inv + 2 * ((size_t)first * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB));
+        for (int e = threadIdx.x; e < fs * TB; e += blockDim.x) Ws[e / TB][e % TB] = ldc<R>(W, e);
+        ws_ready = true;
+        __syncthreads();
+    }
+    for (int step = 0; step < nb; ++step) {
+        const int b = a.backward ? nb - 1 - step : step;
+        const int b0 = b * TB, bs = min(TB, a.n - b0);
+        const bool mine = b >= bb0 && b < bb1;
+        const bool before_mine = a.backward ? b >= bb1 : b < bb0;
+        if (!mine && !before_mine) break;                           // blocks after mine do not touch my rows
+        if (!mine) {
+            prefetch(b0, bs, R0, R1);                               // the factor reads do not wait for the flag
+            if (threadIdx.x == 0) {
+                long it = 0;
+                while (ld_acquire_u32((const unsigned *)(a.flags + b)) != (unsigned)epoch) {
+                    if (++it > (1L << 26) || *(volatile int *)a.err) { ok = 0; dev_error(a.err, M25_DEV_TIMEOUT); break; }
+                    __nanosleep(32);
+                }
+            }
+            __syncthreads();
+            if (!ok) return;
+            for (int e = threadIdx.x; e < bs * nrhs; e += blockDim.x) {       // another CTA's values: past L1
+                const R *p = a.Xout + 2 * ((size_t)(b0 + e / nrhs) * nrhs + e % nrhs);
+                Yb[e / nrhs][e % nrhs] = mk<R>(__ldcg(p), __ldcg(p + 1));
+            }
+            __syncthreads();
+            apply(b0, bs, R0, R1, true);                            // every row of mine comes after it
+            __syncthreads();
+            continue;
+        }
+        // my block: solve it (its inverse staged at the start or after my previous block), publish, apply to my
+        // remaining rows
+        if (!ws_ready) {
+            const R *W = a.inv + 2 * ((size_t)b * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB));
+            for (int e = threadIdx.x; e < bs * TB; e += blockDim.x) Ws[e / TB][e % TB] = ldc<R>(W, e);
+        }
+        ws_ready = false;
+        __syncthreads();
+        for (int e = threadIdx.x; e < bs * nrhs; e += blockDim.x) {
+            int rr = e / nrhs, c = e % nrhs;
+            C acc = mk<R>(0, 0);
+            for (int k = 0; k < bs; ++k) cfma<R>(acc, Ws[k][rr], T[b0 - R0 + k][c]);
+            Yb[rr][c] = acc;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < bs * nrhs; e += blockDim.x)
+            stc<R>(a.Xout, (size_t)(b0 + e / nrhs) * nrhs + e % nrhs, Yb[e / nrhs][e % nrhs]);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) atomicExch(a.flags + b, epoch);
+        // the next own block's inverse, while the rows are updated (Ws is free: this block's y is in Yb)
+        const int nxt = a.backward ? b - 1 : b + 1;
+        if (nxt >= bb0 && nxt < bb1) {
+            const int ns = min(TB, a.n - nxt * TB);
+            const R *W = a.inv + 2 * ((size_t)nxt * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB));
+            for (int e = threadIdx.x; e < ns * TB; e += blockDim.x) Ws[e / TB][e % TB] = ldc<R>(W, e);
+            ws_ready = true;
+        }
+        if (a.backward) apply(b0, bs, R0, b0, false);               // my earlier rows
+        else apply(b0, bs, b0 + bs, R1, false);                     // my later rows
+        __syncthreads();
+    }
+}
+
 // X = P z: the interchanges applied from the last to the first (zlaswp with incx = -1): a permutation built in
 // shared memory by one thread, then the rows gathered
 __global__ void k_perm_from_ipiv(const int *ipiv, int n, int *perm)
@@ -606,53 +780,109 @@ extern "C" int m25_getrf(void *d_A, long lda, int n, int *d_ipiv, int single, in
 }
 
 template <typename R>
-static int getrs_impl(const R *A, long lda, int n, const int *ipiv, R *B, int nrhs, cudaStream_t s)
+static size_t aux_layout(int n, size_t *off_inv, size_t *off_perm, size_t *off_w, size_t *off_flags = nullptr)
 {
-    const int sms = std::max(1, sm_count());
-    const size_t tri_smem = sizeof(cpx<R>) * (TB * (TB + 1) + TB * 16);
-    M25_CHECK(cudaFuncSetAttribute(k_tri_block<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem));
-    for (int i0 = 0; i0 < n; i0 += TB) {                              // U^T y = b
-        int bs = std::min(TB, n - i0);
-        k_tri_block<R><<<1, 256, tri_smem, s>>>(A, lda, n, i0, bs, B, nrhs, 1);
-        M25_LAUNCH_CHECK("k_tri_block");
-        if (i0 + bs < n) {
-            int blocks = std::min(sms * 8, (n - i0 - bs + 7) / 8);
-            k_tri_update<R><<<blocks, 256, 0, s>>>(A, lda, i0, bs, i0 + bs, n, B, nrhs);
-            M25_LAUNCH_CHECK("k_tri_update");
-        }
-    }
-    for (int i0 = ((n - 1) / TB) * TB; i0 >= 0; i0 -= TB) {           // L^T z = y
-        int bs = std::min(TB, n - i0);
-        k_tri_block<R><<<1, 256, tri_smem, s>>>(A, lda, n, i0, bs, B, nrhs, 0);
-        M25_LAUNCH_CHECK("k_tri_block");
-        if (i0 > 0) {
-            int blocks = std::min(sms * 8, (i0 + 7) / 8);
-            k_tri_update<R><<<blocks, 256, 0, s>>>(A, lda, i0, bs, 0, i0, B, nrhs);
-            M25_LAUNCH_CHECK("k_tri_update");
-        }
-    }
-    // X = P z
-    int *perm;
-    R *tmp;
-    M25_CHECK(cudaMallocAsync(&perm, sizeof(int) * n, s));
-    M25_CHECK(cudaMallocAsync(&tmp, sizeof(R) * 2 * (size_t)n * nrhs, s));
-    M25_REQUIRE(sizeof(int) * (size_t)n <= 200 * 1024, "m25_getrs: n above 51200");
+    const size_t nb = (n + TB - 1) / TB;
+    size_t o = 0;
+    *off_inv = o; o += nb * 2 * TB * TB * sizeof(cpx<R>); o = (o + 255) / 256 * 256;
+    *off_perm = o; o += sizeof(int) * (size_t)n; o = (o + 255) / 256 * 256;
+    *off_w = o; o += 2 * (size_t)n * 16 * sizeof(cpx<R>); o = (o + 255) / 256 * 256;
+    if (off_flags) *off_flags = o;
+    o += sizeof(int) * (2 * nb + 32);                  // flags of the two solves, then the epoch counter
+    return o;
+}
+
+extern "C" size_t m25_getrs_aux_bytes(int n, int single)
+{
+    size_t a, b, c;
+    return single ? aux_layout<float>(n, &a, &b, &c) : aux_layout<double>(n, &a, &b, &c);
+}
+
+template <typename R>
+static size_t trsv_smem(int n, int G)
+{
+    const int nb = (n + TB - 1) / TB, per = (nb + G - 1) / G;
+    return sizeof(cpx<R>) * (TB * (TB + 1) + TB * 16 + (size_t)per * TB * 16);
+}
+
+template <typename R>
+static int getrs_prepare_impl(const R *A, long lda, int n, const int *ipiv, unsigned char *aux, size_t aux_bytes,
+                              cudaStream_t s)
+{
+    size_t oi, op, ow, of;
+    M25_REQUIRE(aux_bytes >= aux_layout<R>(n, &oi, &op, &ow, &of), "m25_getrs_prepare: aux buffer too small");
+    const int nb = (n + TB - 1) / TB;
+    const size_t ismem = 2 * sizeof(cpx<R>) * TB * (TB + 1);
+    M25_CHECK(cudaFuncSetAttribute(k_block_inverses<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem));
+    k_block_inverses<R><<<nb, TB, ismem, s>>>(A, lda, n, (R *)(aux + oi));
+    M25_LAUNCH_CHECK("k_block_inverses");
+    M25_REQUIRE(sizeof(int) * (size_t)n <= 200 * 1024, "m25_getrs_prepare: n above 51200");
     M25_CHECK(cudaFuncSetAttribute(k_perm_from_ipiv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(sizeof(int) * n)));
-    k_perm_from_ipiv<<<1, 1024, sizeof(int) * n, s>>>(ipiv, n, perm);
+    k_perm_from_ipiv<<<1, 1024, sizeof(int) * n, s>>>(ipiv, n, (int *)(aux + op));
     M25_LAUNCH_CHECK("k_perm_from_ipiv");
-    M25_CHECK(cudaMemcpyAsync(tmp, B, sizeof(R) * 2 * (size_t)n * nrhs, cudaMemcpyDeviceToDevice, s));
-    long tot = (long)n * nrhs;
-    k_gather_rows<R><<<(tot + 255) / 256, 256, 0, s>>>(tmp, B, perm, n, nrhs);
-    M25_LAUNCH_CHECK("k_gather_rows");
-    M25_CHECK(cudaFreeAsync(perm, s));
-    M25_CHECK(cudaFreeAsync(tmp, s));
+    M25_CHECK(cudaMemsetAsync(aux + of, 0, sizeof(int) * (2 * nb + 32), s));
     return M25_OK;
+}
+
+template <typename R>
+static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B, int nrhs, cudaStream_t s)
+{
+    size_t oi, op, ow, of;
+    aux_layout<R>(n, &oi, &op, &ow, &of);
+    const R *inv = (const R *)(aux + oi);
+    const int *perm = (const int *)(aux + op);
+    R *W1 = (R *)(aux + ow), *W2 = W1 + 2 * (size_t)n * 16;
+    const int nb = (n + TB - 1) / TB;
+    int *flags = (int *)(aux + of), *epoch = flags + 2 * nb;
+    const int G = std::max(1, std::min(sm_count(), nb));
+    const size_t sm = trsv_smem<R>(n, G);
+    M25_REQUIRE(sm <= 200 * 1024, "m25_getrs_aux: n too large for the persistent solve");
+    M25_CHECK(cudaFuncSetAttribute(k_trsv_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_bump_epoch<<<1, 1, 0, s>>>(epoch);                                    // this call's flag value
+    M25_LAUNCH_CHECK("k_bump_epoch");
+    int *err = m25_dev_err_word();
+    TrsvArgs<R> fa{A, lda, n, nb, inv, B, W1, nrhs, 0, flags, epoch, err};          // U^T y = b: B -> W1
+    void *fargs[] = {&fa};
+    M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), fargs, sm, s));
+    m25_note_launch();
+    TrsvArgs<R> ba{A, lda, n, nb, inv, W1, W2, nrhs, 1, flags + nb, epoch, err};    // L^T z = y: W1 -> W2
+    void *bargs[] = {&ba};
+    M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), bargs, sm, s));
+    m25_note_launch();
+    long tot = (long)n * nrhs;                                              // X = P z
+    k_gather_rows<R><<<(tot + 255) / 256, 256, 0, s>>>(W2, B, perm, n, nrhs);
+    M25_LAUNCH_CHECK("k_gather_rows");
+    return M25_OK;
+}
+
+extern "C" int m25_getrs_prepare(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
+                                 size_t aux_bytes, void *stream)
+{
+    M25_REQUIRE(d_LU && d_ipiv && d_aux && n >= 1 && lda >= n, "m25_getrs_prepare: LU, ipiv, aux, n >= 1");
+    return single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes, S(stream))
+                  : getrs_prepare_impl<double>((const double *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes,
+                                               S(stream));
+}
+
+extern "C" int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void *d_aux, void *d_B, int nrhs, void *stream)
+{
+    M25_REQUIRE(d_LU && d_aux && d_B && n >= 1 && lda >= n, "m25_getrs_aux: LU, aux, B, n >= 1");
+    M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs_aux: 1 to 16 right-hand sides a call");
+    return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, S(stream))
+                  : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)d_aux, (double *)d_B, nrhs,
+                                           S(stream));
 }
 
 extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream)
 {
     M25_REQUIRE(d_LU && d_ipiv && d_B && n >= 1 && lda >= n, "m25_getrs: LU, ipiv, B, n >= 1");
     M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs: 1 to 16 right-hand sides a call");
-    return single ? getrs_impl<float>((const float *)d_LU, lda, n, d_ipiv, (float *)d_B, nrhs, S(stream))
-                  : getrs_impl<double>((const double *)d_LU, lda, n, d_ipiv, (double *)d_B, nrhs, S(stream));
+    const size_t bytes = m25_getrs_aux_bytes(n, single);
+    void *aux = nullptr;
+    M25_CHECK(cudaMallocAsync(&aux, bytes, S(stream)));
+    int rc = m25_getrs_prepare(d_LU, lda, n, d_ipiv, single, aux, bytes, stream);
+    if (!rc) rc = m25_getrs_aux(d_LU, lda, n, single, aux, d_B, nrhs, stream);
+    cudaError_t fe = cudaFreeAsync(aux, S(stream));
+    if (!rc && fe != cudaSuccess) return m25_cuda_status(fe, "cudaFreeAsync");
+    return rc;
 }

@@ -99,6 +99,7 @@ class DeviceGeometry:
                                    c_double(geo.near_fac), P(off), ctypes.byref(total), P(self.nP), P(self.nQ), s),
               'm25_near_pairs')
         self.npairs = n
+        self.off = off                                  # pairs of triangle p: off[p] .. off[p + 1] (sorted by p)
 
     def _via_setup(self):
         """Index lists of the via blocks, built once (sim.py:786-814): the fans' divergence dF as CSR by chain,

@@ -27,6 +27,7 @@ c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
 MIXED_MAX_ITER = 30          # fast.py:255
 FRESH_STALL = (4, 0.1)       # fast.py:256
 MIXED_RTOL = 1e-6            # fast.py:366 (FastOperator.mixed_tol)
+PREDICT_AFTER = 6            # iterations after which a fresh factor's refinement may be judged hopeless (gmres_batched)
 
 
 class SolveFailed(RuntimeError):
@@ -76,7 +77,9 @@ class DirectSolver:
         geo, dg = self.geo, self.dg
         N, Ne = geo.N, geo.Ne
         single = precision == 'mixed'
+        t0 = time.perf_counter()
         self.setup(f, single=single)
+        self._t('tables', t0)
         tb, s = self.tabs, self.s
         qcorr = self._buf('qcorr', (max(1, dg.npairs),), torch.complex128)
         if not single:
@@ -88,7 +91,9 @@ class DirectSolver:
                                  ctypes.byref(dg.quad), P(dg.nP), P(dg.nQ), c_long(dg.npairs), c_double(self.w), s),
                   'm25_near')
             dg.stat_ready = True
+            t0 = time.perf_counter()
             self.vias.assemble(Z, N, qcorr)
+            self._t('vias', t0)
             return Z
         Z = self._buf('Z64', (N, N), torch.complex64)
         check(lib().m25_fill_far(P(Z), c_long(N), c_int(1), ctypes.byref(dg.mesh), None, ctypes.byref(tb.tables32),
@@ -106,7 +111,9 @@ class DirectSolver:
               'm25_coo_add_c64')
         self.Bv = self._buf('Bv', (max(1, Ne * geo.Nv),), torch.complex128)
         self.Cv = self._buf('Cv', (max(1, geo.Nv * geo.Nv),), torch.complex128)
+        t0 = time.perf_counter()
         self.vias.assemble(None, N, qcorr, Z64=Z, B=self.Bv, C=self.Cv)
+        self._t('vias', t0)
         return Z
 
     # ---- the exact double-precision operator (fast.py:571-593) --------------------------------------------------------
@@ -121,8 +128,8 @@ class DirectSolver:
         Ye = torch.empty((Ne, k), dtype=torch.complex128, device='cuda')
         check(lib().m25_matvec_far_multi(P(Xe), c_int(k), P(Ye), P(work), ctypes.byref(dg.mesh),
                                          ctypes.byref(self.tabs.tables), c_double(self.w), s), 'm25_matvec_far_multi')
-        check(lib().m25_coo_spmm(P(self.ri), P(self.ci), P(self.vv), c_long(9 * dg.npairs), P(Xe), c_int(k), P(Ye), s),
-              'm25_coo_spmm')
+        check(lib().m25_near_spmm_rows(ctypes.byref(dg.mesh), P(dg.off), P(dg.nQ), P(self.vv), P(Xe), c_int(k), P(Ye),
+                                       s), 'm25_near_spmm_rows')
         Y[:Ne] = Ye
         if geo.Nv:
             check(lib().m25_border_mv(P(self.Bv), P(self.Cv), c_int(Ne), c_int(geo.Nv), P(X), c_int(k), P(Y), s),
@@ -161,6 +168,11 @@ class DirectSolver:
         b.record(st)
         _lib.sync_check(self.stream, 'm25_getrf')
         self.last_lu_ms = a.elapsed_time(b)                # the factorisation alone, on its stream
+        # the solves' diagonal-block inverses and row permutation, once per factor
+        nbytes = int(lib().m25_getrs_aux_bytes(c_int(N), c_int(int(single))))
+        self.aux = self._buf('getrs_aux_%d' % single, (nbytes,), torch.uint8)
+        check(lib().m25_getrs_prepare(P(Z), c_long(N), c_int(N), P(ipiv), c_int(int(single)), P(self.aux),
+                                      ctypes.c_size_t(nbytes), self.s), 'm25_getrs_prepare')
         return ipiv
 
     def _lu_solve(self, Z, ipiv, R, single):
@@ -169,12 +181,14 @@ class DirectSolver:
         if single:
             R64 = torch.empty((N, k), dtype=torch.complex64, device='cuda')
             check(lib().m25_convert(P(R), c_int(0), P(R64), c_long(N * k), self.s), 'm25_convert')
-            check(lib().m25_getrs(P(Z), c_long(N), c_int(N), P(ipiv), c_int(1), P(R64), c_int(k), self.s), 'm25_getrs')
+            check(lib().m25_getrs_aux(P(Z), c_long(N), c_int(N), c_int(1), P(self.aux), P(R64), c_int(k), self.s),
+                  'm25_getrs_aux')
             X = torch.empty((N, k), dtype=torch.complex128, device='cuda')
             check(lib().m25_convert(P(R64), c_int(1), P(X), c_long(N * k), self.s), 'm25_convert')
             return X
         X = R.clone()
-        check(lib().m25_getrs(P(Z), c_long(N), c_int(N), P(ipiv), c_int(0), P(X), c_int(k), self.s), 'm25_getrs')
+        check(lib().m25_getrs_aux(P(Z), c_long(N), c_int(N), c_int(0), P(self.aux), P(X), c_int(k), self.s),
+              'm25_getrs_aux')
         return X
 
     def solve_direct(self, f, E, block=1024, precision='double'):
@@ -203,8 +217,17 @@ class DirectSolver:
             X = self._scale(Y, rows=dsc)
             self._t('solve', t0)
             return X
-        A = lambda V: self._scale(self.matvec_exact(self._scale(V, rows=dsc)), rows=dsc)
-        M = lambda R: self._lu_solve(Z, ipiv, R, True)
+        def A(V):
+            t = time.perf_counter()
+            Y = self._scale(self.matvec_exact(self._scale(V, rows=dsc)), rows=dsc)
+            self._t('refine_matvec', t)
+            return Y
+
+        def M(R):
+            t = time.perf_counter()
+            X = self._lu_solve(Z, ipiv, R, True)
+            self._t('refine_precond', t)
+            return X
         Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, 1, FRESH_STALL)
         self._t('refine', t0)
         if not ok:
@@ -279,6 +302,15 @@ class DirectSolver:
                 if stall is not None and j + 1 >= stall[0] and (np.abs(g[j + 1])[live] > stall[1] * bn[act][live]).any():
                     last[live], stalled = j, True
                     break
+                if stall is not None and j + 1 >= PREDICT_AFTER:
+                    # the residual's geometric rate so far, extrapolated to the last iteration: a column that would
+                    # still be 10x above the tolerance there ends the refinement now (its iterations would be lost:
+                    # the caller solves in double precision either way)
+                    r0, rj = np.abs(g[0])[live], np.abs(g[j + 1])[live]
+                    rate = (rj / np.maximum(r0, 1e-300)) ** (1.0 / (j + 1))
+                    if (rj * rate ** (restart - j - 1) > 10 * rtol * bn[act][live]).any():
+                        last[live], stalled = j, True
+                        break
             ys = []
             for c in range(ka):
                 m = last[c] + 1

@@ -77,9 +77,39 @@ def time_update(M, N, K, reps=5):
                 tflops_tf32_issued=3 * 8.0 * M * N * K / ms / 1e9)
 
 
+def time_solve(n, nrhs=8, single=True, reps=5):
+    """The triangular solves with a factor (m25_getrs_aux, diagonal-block inverses prepared once)."""
+    dtype = torch.complex64 if single else torch.complex128
+    Z = random_matrix(n, dtype)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(lib().m25_getrf_workspace(n, int(single)))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    check(lib().m25_getrf(P(Z), ctypes.c_long(n), n, P(ipiv), int(single), int(single), P(work), ctypes.c_size_t(nb),
+                          _lib.stream_ptr()), 'm25_getrf')
+    na = int(lib().m25_getrs_aux_bytes(n, int(single)))
+    aux = torch.empty(na, dtype=torch.uint8, device='cuda')
+    check(lib().m25_getrs_prepare(P(Z), ctypes.c_long(n), n, P(ipiv), int(single), P(aux), ctypes.c_size_t(na),
+                                  _lib.stream_ptr()), 'm25_getrs_prepare')
+    B = random_matrix(max(n, nrhs), dtype, seed=3)[:n, :nrhs].contiguous()
+    s = torch.cuda.current_stream()
+    out = []
+    for r in range(reps + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        check(lib().m25_getrs_aux(P(Z), ctypes.c_long(n), n, int(single), P(aux), P(B), nrhs, _lib.stream_ptr()),
+              'm25_getrs_aux')
+        b.record(s)
+        _lib.sync_check()
+        if r:
+            out.append(a.elapsed_time(b))
+    ms = float(np.median(out))
+    return dict(n=n, nrhs=nrhs, single=single, ms=ms, factor_GBps=n * n * (8 if single else 16) / ms / 1e6)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--update', type=int, nargs=3, default=None, metavar=('M', 'N', 'K'))
+    ap.add_argument('--solve', type=int, default=0)
     ap.add_argument('--lu', type=int, default=0)
     ap.add_argument('--single', action='store_true')
     ap.add_argument('--tf32', action='store_true')
@@ -90,6 +120,8 @@ def main():
         print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
     if a.update:
         print(json.dumps(time_update(*a.update, reps=a.reps)))
+    if a.solve:
+        print(json.dumps(time_solve(a.solve, single=a.single, reps=a.reps)))
 
 
 if __name__ == '__main__':
