@@ -87,11 +87,65 @@ int m25_spectral(const double *d_kr, int npts, double w, int nl, const double *h
  * kr, dk complex128[npts]; W complex128[ns*npts]; rho f64[nr]; out complex128[ns*nr]. */
 int m25_hankel(const double *d_kr, const double *d_dk, int npts, const double *d_W, int ns, const double *d_rho,
                int nr, double *d_out, void *stream);
+/* out[s, i] = sum_k J0(rho_i kr_k) W[s, k] over real kr f64[nk] (hankel_real, mom25d_core.cpp:1430-1454);
+ * W complex128[ns*nk], out complex128[ns*nr], ns <= 16. */
+int m25_hankel_real(const double *d_rho, int nr, const double *d_kr, int nk, const double *d_W, int ns,
+                    double *d_out, void *stream);
 /* Not-a-knot cubic spline through (x[i], y[s, i]), i < n, evaluated at nfine uniform points from 0 step dx
  * (via.py:111-123 Table1D, SciPy CubicSpline). y complex128[ns*n]; out: complex128 or (single) complex64
  * [ns*nfine]; out_stride: elements between rows. */
 int m25_spline_uniform(const double *d_x, const double *d_y, int ns, int n, double dx, int nfine, void *d_out,
                        int single, long out_stride, long out_offset_elems, int out_interleave, void *stream);
+/* The spectral kernels of npair (<= 64) interface pairs with their singular parts subtracted in the spectral
+ * domain before the Hankel transform (GreenTableML.__init__ / extracted, multilayer.py:260-299): per pair i,
+ * next[i] (0..2) extracted terms of distance d[2i + j] and coefficients cA, cq (complex128, host [npair*2]).
+ * d_pairs_scratch: m25_pair_record_bytes() device bytes. Synchronous in its host-to-device copy of the records. */
+int m25_spectral_extracted(const double *d_kr, int npts, double w, int nl, const double *h_h, const double *h_eps,
+                           int top_open, const double *h_top_eps, int npair, const int *h_o, const int *h_s,
+                           const int *h_next, const double *h_d, const double *h_cA, const double *h_cq,
+                           double *d_GA, double *d_GQ, void *d_pairs_scratch, void *stream);
+size_t m25_pair_record_bytes(void);
+/* The spectral kernels G_A, G_q of one interface pair (o, s) at npts (kr, w) points, each point its own angular
+ * frequency w[i] (real): the large-kr limits that give the extraction coefficients (multilayer.py:271-287). */
+int m25_spectral_points(const double *d_kr, const double *d_w, int npts, int nl, const double *h_h,
+                        const double *h_eps, int top_open, const double *h_top_eps, int o, int s, double *d_ga,
+                        double *d_gq, void *stream);
+
+/* ---- via kernels (via.py:127-235 TMNetwork / ViaKernels, sim.py:786-872 _via_blocks) --------------------------- */
+/* The via spectra on the contour: nd (<= 32) D spectra (strip interface dk[i], via span dspan[2i..2i+1]) then
+ * nr (<= 32) R spectra (span rm[2i..] against span rn[2i..], without the homogeneous term) (via.py:205-220);
+ * out complex128[(nd + nr) * npts], row-major by spectrum. */
+int m25_via_spectra(const double *d_kr, int npts, double w, int nl, const double *h_h, const double *h_eps,
+                    int top_open, const double *h_top_eps, int nd, const int *h_dk, const int *h_dspan, int nr,
+                    const int *h_rm, const int *h_rn, double *d_out, void *stream);
+/* The analytic homogeneous (K0) term of the via-via kernel at n distances rho for the layers in layer_mask
+ * (via.py:222-235 ViaKernels.homog); out complex128[n]. */
+int m25_via_homog(const double *d_rho, int n, double w, int nl, const double *h_h, const double *h_eps,
+                  int top_open, const double *h_top_eps, unsigned layer_mask, double *d_out, void *stream);
+/* QF[row[k], col[k]] += qcorr[pair[k]]: the near pairs' G_q corrections on the fan columns (fast.py:501-503).
+ * QF complex128[Nt*nf]. */
+int m25_via_qcorr(double *d_QF, int nf, const int *d_pair, const int *d_row, const int *d_col, int n,
+                  const double *d_qcorr, void *stream);
+/* T[t, n] = sum over chain n's fan entries (fj[k], fw[k]), k in ptr[n]..ptr[n+1], of QF[t, fj[k]] fw[k]
+ * (the fan charges dF of sim.py:840-849); T complex128[Nt*Nv]. */
+int m25_via_fan_T(const double *d_QF, int Nt, int nf, const int *d_ptr, const int *d_fj, const double *d_fw, int Nv,
+                  double *d_T, void *stream);
+/* c[t, n] = sum over the 6 points of triangle t of D(|P6 - V_n|) W6, D the table dtab[lt[t] * nspan + span_of[n]]
+ * of D complex128[ntables*nfine] (radial_table_sum per interface and span, mom25d_core.cpp:1269-1298). */
+int m25_via_radial(const double *d_P6, const double *d_W6, const int *d_lt, int Nt, const double *d_vx,
+                   const double *d_vy, const int *d_span_of, int Nv, const double *d_D, const int *d_dtab, int nspan,
+                   long nfine, double dr, double *d_c, void *stream);
+/* The via border: B = D^T (T / jw + c) (Ne x Nv) and C = dF^T T / jw + R (Nv x Nv) (sim.py:850-872), written into
+ * the bordered Z (complex128 d_Z and / or complex64 d_Z64, leading dimension ld >= Ne + Nv: columns and rows
+ * Ne..Ne+Nv-1) and / or separate d_B, d_C buffers; null destinations are skipped. */
+int m25_via_assemble(const double *d_T, const double *d_c, const int *d_F, const int *d_ptr, const int *d_fj,
+                     const double *d_fw, int Nv, const double *d_R, const m25_mesh *g, double w, double *d_Z,
+                     float *d_Z64, long ld, double *d_B, double *d_C, void *stream);
+/* R[m, n] += vals[k] (or the lerp of tab at dd[k] when d_tab != NULL) + homog[k], and R[n, m] the same, for the
+ * np via pairs (pm[k] <= pn[k]) (the via-via R kernel, via.py:188-221); R complex128[Nv*Nv]. */
+int m25_via_pairs(const int *d_pm, const int *d_pn, const double *d_dd, int np, const double *d_vals,
+                  const double *d_homog, const double *d_tab, long nfine, double dr, int Nv, double *d_R,
+                  void *stream);
 
 /* ---- fill (mom25d_core.cpp) ------------------------------------------------------------------------------------ */
 /* Centroid-rule far field of every edge pair into Z (Ne x Ne block of a row-major N x ld matrix), both
@@ -131,6 +185,34 @@ int m25_matvec_far_multi(const double *d_X, int K, double *d_Y, double *d_work, 
  * mom25d_core.cpp:1563-1580; _equilibrate fast.py:294-305). dsc: if d_dsc_out != NULL, first computes
  * d = 1 / sqrt(|Z_ii| + 1e-300) into it and uses that. */
 int m25_equilibrate(double *d_Z, long n, long ld, const double *d_d, double *d_dsc_out, float *d_Z64, void *stream);
+/* The same for a complex64 Z (the mixed-precision fill writes complex64 directly): d from its diagonal into
+ * d_dsc_out (f64[n]), Z <- diag(d) Z diag(d). */
+int m25_equilibrate_c64(float *d_Z, long n, long ld, double *d_dsc_out, void *stream);
+
+/* ---- the exact FP64 operator and the refinement's vector kernels (fast.py:571-593, 1437-1500) ----------------- */
+/* Vectors are N x k row-major complex128 (one column per right-hand side). */
+/* out[c] += sum_n conj(V[n, c]) W[n, c] (out zeroed by the caller). */
+int m25_dotc_cols(const double *d_V, const double *d_W, long N, int k, double *d_out, void *stream);
+/* W[n, c] += V[n, c] a[c]. */
+int m25_axpy_cols(double *d_W, const double *d_V, const double *d_a, long N, int k, void *stream);
+/* Y[n, c] = X[n, c] s[c] (times rows[n] when d_rows != NULL); s complex128[k] or NULL for 1. */
+int m25_scale_cols(double *d_Y, const double *d_X, const double *d_s, const double *d_rows, long N, int k,
+                   void *stream);
+/* n complex numbers complex128 -> complex64 (in_single = 0) or complex64 -> complex128 (in_single = 1). */
+int m25_convert(const void *d_in, int in_single, void *d_out, long n, void *stream);
+/* Y[ri[s], c] += vv[s] X[ci[s], c] over COO triplets (ri < 0 unused; near_matvec, mom25d_core.cpp:540-556). */
+int m25_coo_spmm(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, const double *d_X, int k,
+                 double *d_Y, void *stream);
+/* The same product row by row without atomics (deterministic): the triplets of m25_near mode 2 in pair order,
+ * off int64[Nt+1] the pairs of each observation triangle, Q the source triangles. */
+int m25_near_spmm_rows(const m25_mesh *g, const long long *d_off, const int *d_Q, const double *d_vv,
+                       const double *d_X, int k, double *d_Y, void *stream);
+/* Z (complex64, ld) += vv at (ri, ci): the near field into the mixed-precision matrix. */
+int m25_coo_add_c64(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, float *d_Z, long ld,
+                    void *stream);
+/* The via border of Z X (fast.py:580-586): Y[:Ne] += B X[Ne:], Y[Ne:] = B^T X[:Ne] + C X[Ne:]. */
+int m25_border_mv(const double *d_B, const double *d_C, int Ne, int Nv, const double *d_X, int k, double *d_Y,
+                  void *stream);
 
 /* ---- complex dense LU (gpu.py:28-110 backend factor / solve / download; fast.py:318-358 _lu / _lu_solve) ------- */
 /* Workspace bytes m25_getrf needs for an n x n factorisation. */
@@ -144,10 +226,27 @@ int m25_getrf(void *d_A, long lda, int n, int *d_ipiv, int single, int tf32, voi
 /* Solves Z X = B with the factor of Z^T (lu_solve(..., trans=1)); B (row-major n x nrhs, complex in the factor's
  * precision) overwritten by X. */
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);
+/* The solves split for a factor that is solved with many times (the refinement's preconditioner, the backend's
+ * solve(R)): m25_getrs_prepare inverts the factor's diagonal blocks once into d_aux (m25_getrs_aux_bytes) and
+ * keeps the pivots there; m25_getrs_aux then solves like m25_getrs from d_aux. d_aux belongs to one factor. */
+size_t m25_getrs_aux_bytes(int n, int single);
+int m25_getrs_prepare(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
+                      size_t aux_bytes, void *stream);
+int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void *d_aux, void *d_B, int nrhs, void *stream);
+/* The LU's tensor-core trailing update alone: C (M x N complex64, column-major, ld) -= L (M x K) U (K x N), both
+ * column-major with leading dimension ld, as 3xTF32 products on tcgen05. work: split operands. */
+int m25_cgemm_update_tf32(float *d_C, long ld, int M, int N, int K, const float *d_L, const float *d_U, void *d_work,
+                          size_t work_bytes, void *stream);
+/* 1 when the library carries the tensor-core (tcgen05) update. */
+int m25_umma_available(void);
 
 /* ---- small helpers ------------------------------------------------------------------------------------------------ */
 /* J_n(z) elementwise for complex z, n = 0, 1, 2 (bessel_jn_complex, mom25d_core.cpp:1545-1558). */
 int m25_bessel_jn_complex(int order, const double *d_z, long count, double *d_out, void *stream);
+/* Synchronises stream and turns a pending kernel error (or a device-side check, M25_EDEVICE) into a status. */
+int m25_sync_check(void *stream);
+/* How many kernels this library has launched in the process (a counter for measurements). */
+long long m25_launch_count(void);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,7 @@ def lib():
         L.m25_getrs_aux_bytes.restype = ctypes.c_size_t
         L.m25_getrf_workspace.argtypes = [ctypes.c_int, ctypes.c_int]
         L.m25_pair_record_bytes.restype = ctypes.c_size_t
+        L.m25_launch_count.restype = ctypes.c_longlong
         _lib = L
     return _lib
 

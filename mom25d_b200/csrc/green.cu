@@ -331,7 +331,9 @@ __global__ void k_via_homog(const double *rho, int n, double w, Stack st, unsign
 // ---- Hankel transform (via.py:90-108): out[s, i] = (1/2pi) sum_k J0(rho_i kr_k) W[s, k] kr_k dk_k -------------------
 // One block per radius; the contour split over the threads (J0 of a real argument: the CUDA math library's j0;
 // on the lifted part the complex series above); then a block reduction per spectrum.
-template <int NS>
+// RAW: the bare sum over real kr (hankel_real, mom25d_core.cpp:1430-1454): out[s, i] = sum_k J0(rho_i kr_k) W[s, k],
+// kr_ real f64[npts], no dk, no 1 / 2 pi.
+template <int NS, bool RAW = false>
 __global__ void __launch_bounds__(256) k_hankel(const double *kr_, const double *dk_, int npts, const double *W, int ns,
                                                 const double *rho, double *out, int nr)
 {
@@ -341,9 +343,14 @@ __global__ void __launch_bounds__(256) k_hankel(const double *kr_, const double 
     zd acc[NS];
     for (int s = 0; s < NS; ++s) acc[s] = mk<double>(0, 0);
     for (int k = threadIdx.x; k < npts; k += blockDim.x) {
-        zd kr = ldc<double>(kr_, k), dk = ldc<double>(dk_, k);
-        zd J = fabs(kr.y) < 1e-300 ? mk<double>(j0(r * kr.x), 0) : jn_complex(0, kr * r);
-        zd f = J * (kr * dk);
+        zd f;
+        if (RAW) {
+            f = mk<double>(j0(r * kr_[k]), 0);
+        } else {
+            zd kr = ldc<double>(kr_, k), dk = ldc<double>(dk_, k);
+            zd J = fabs(kr.y) < 1e-300 ? mk<double>(j0(r * kr.x), 0) : jn_complex(0, kr * r);
+            f = J * (kr * dk);
+        }
         for (int s = 0; s < NS; ++s)
             if (s < ns) acc[s] += f * ldc<double>(W, (size_t)s * npts + k);
     }
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(256) k_hankel(const double *kr_, const double 
     if (threadIdx.x < NS && threadIdx.x < ns) {
         zd t = mk<double>(0, 0);
         for (int j = 0; j < (int)(blockDim.x / 32); ++j) t += red[j][threadIdx.x];
-        stc<double>(out, (size_t)threadIdx.x * nr + i, t * (1.0 / (2 * 3.14159265358979323846)));
+        stc<double>(out, (size_t)threadIdx.x * nr + i, RAW ? t : t * (1.0 / (2 * 3.14159265358979323846)));
     }
 }
 
@@ -569,6 +576,18 @@ extern "C" int m25_hankel(const double *d_kr, const double *d_dk, int npts, cons
     if (ns <= 4) k_hankel<4><<<nr, 256, 0, S(stream)>>>(d_kr, d_dk, npts, d_W, ns, d_rho, d_out, nr);
     else if (ns <= 8) k_hankel<8><<<nr, 256, 0, S(stream)>>>(d_kr, d_dk, npts, d_W, ns, d_rho, d_out, nr);
     else k_hankel<16><<<nr, 256, 0, S(stream)>>>(d_kr, d_dk, npts, d_W, ns, d_rho, d_out, nr);
+    M25_LAUNCH_CHECK("k_hankel");
+    return M25_OK;
+}
+
+extern "C" int m25_hankel_real(const double *d_rho, int nr, const double *d_kr, int nk, const double *d_W, int ns,
+                               double *d_out, void *stream)
+{
+    M25_REQUIRE(ns >= 1 && ns <= 16, "m25_hankel_real: 1 to 16 rows of W a call");
+    if (!nr) return M25_OK;
+    if (ns <= 4) k_hankel<4, true><<<nr, 256, 0, S(stream)>>>(d_kr, nullptr, nk, d_W, ns, d_rho, d_out, nr);
+    else if (ns <= 8) k_hankel<8, true><<<nr, 256, 0, S(stream)>>>(d_kr, nullptr, nk, d_W, ns, d_rho, d_out, nr);
+    else k_hankel<16, true><<<nr, 256, 0, S(stream)>>>(d_kr, nullptr, nk, d_W, ns, d_rho, d_out, nr);
     M25_LAUNCH_CHECK("k_hankel");
     return M25_OK;
 }
