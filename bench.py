@@ -136,6 +136,24 @@ def cpu_reference(geo, n_lu=6000):
     return 1.0 / total, cores, sample, kind, t
 
 
+# ---- replicas: the frequency split and the max over ranks -----------------------------------------------------------
+def rank_frequencies(rank, world):
+    """This rank's frequencies: the sweep in a strided order (step i: FREQS[8 i mod 21]), so that a run of fewer
+    than 21 steps samples the whole band rather than its low end; rank r takes every world-th from position r."""
+    order = [float(FREQS[(8 * i) % len(FREQS)]) for i in range(len(FREQS))]
+    return [f for i, f in enumerate(order) if i % world == rank]
+
+
+def max_over_ranks(values, world, device):
+    """Element-wise max of a list of floats over the ranks (the timing rule); the list itself at world = 1."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 # ---- the GPU arm ----------------------------------------------------------------------------------------------------
 def run_gpu(args, rank, world):
     import torch
@@ -148,10 +166,7 @@ def run_gpu(args, rank, world):
     sim = Simulation.from_board(bd, precision='mixed')
     geo = sim.geo
     ds = sim.fast
-    # the sweep's frequencies in a strided order (step i: FREQS[8 i mod 21]), so a run of fewer than 21 steps
-    # samples the whole band rather than its low end; ranks take every world-th
-    order = [FREQS[(8 * i) % len(FREQS)] for i in range(len(FREQS))]
-    mine = [f for i, f in enumerate(order) if i % world == rank]
+    mine = rank_frequencies(rank, world)
     E_host = torch.from_numpy(geo.excitation()).pin_memory()
     E_dev = E_host.to('cuda')
     stream = torch.cuda.current_stream()
@@ -214,10 +229,7 @@ def run_gpu(args, rank, world):
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = e0.elapsed_time(e1) / 1000.0
-    times = torch.tensor([t_dev, t_e2e, sum(lat64) / 1000.0], dtype=torch.float64, device='cuda')
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    t_dev, t_e2e, t64 = times.tolist()
+    t_dev, t_e2e, t64 = max_over_ranks([t_dev, t_e2e, sum(lat64) / 1000.0], world, 'cuda')
     if rank != 0:
         return None
     N = geo.N
