@@ -233,6 +233,19 @@ size_t m25_getrs_aux_bytes(int n, int single);
 int m25_getrs_prepare(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
                       size_t aux_bytes, void *stream);
 int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void *d_aux, void *d_B, int nrhs, void *stream);
+/* m25_getrs without device allocation (no counterpart in the reference). m25_getrs takes its scratch from the
+ * stream-ordered allocator at every call; this variant uses a fixed file-scope device array of
+ * M25_GETRS_NOALLOC_MAX_BYTES instead, for callers that must not have the library take device memory during a
+ * call: a serving loop that admits requests by a fixed HBM budget, or a process whose memory is all reserved up
+ * front. Same arguments and results as m25_getrs. Limit: n with m25_getrs_aux_bytes(n, single) above
+ * M25_GETRS_NOALLOC_MAX_BYTES (about n = 26,000 complex64, 13,000 complex128) is rejected with M25_EINVAL and a
+ * message. The first call on a device does the setup (it looks up the array's device address); make it before
+ * any stream capture. The array is one per device and process: calls that overlap (other streams, other host
+ * threads on the same device) race on it and must be serialised by the caller. A bounded wait that gave up is
+ * reported by m25_sync_check, as for the other kernels. */
+#define M25_GETRS_NOALLOC_MAX_BYTES (32u << 20)
+int m25_getrs_noalloc(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs,
+                      void *stream);
 /* The LU's tensor-core trailing update alone: C (M x N complex64, column-major, ld) -= L (M x K) U (K x N), both
  * column-major with leading dimension ld, as 3xTF32 products on tcgen05. work: split operands. */
 int m25_cgemm_update_tf32(float *d_C, long ld, int M, int N, int K, const float *d_L, const float *d_U, void *d_work,

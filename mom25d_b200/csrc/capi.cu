@@ -28,6 +28,8 @@ int m25_cuda_status(cudaError_t e, const char *where)
 static int *g_dev_err[64];
 static std::mutex g_mu;
 
+int *m25_noalloc_status_word();
+
 int *m25_dev_err_word()
 {
     int dev = 0;
@@ -69,6 +71,11 @@ extern "C" int m25_sync_check(void *stream)
     if (!w) { g_err = "m25_sync_check: no device error word"; return M25_ECUDA; }
     int code = 0;
     M25_CHECK(cudaMemcpy(&code, w, sizeof(int), cudaMemcpyDeviceToHost));
+    int *nw = m25_noalloc_status_word();               // m25_getrs_noalloc's own word, where it has run
+    if (!code && nw) {
+        M25_CHECK(cudaMemcpy(&code, nw, sizeof(int), cudaMemcpyDeviceToHost));
+        if (code) w = nw;
+    }
     if (code) {
         M25_CHECK(cudaMemset(w, 0, sizeof(int)));
         char buf[128];

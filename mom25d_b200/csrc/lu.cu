@@ -825,7 +825,7 @@ static int getrs_prepare_impl(const R *A, long lda, int n, const int *ipiv, unsi
 }
 
 template <typename R>
-static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B, int nrhs, cudaStream_t s)
+static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B, int nrhs, cudaStream_t s, int *err)
 {
     size_t oi, op, ow, of;
     aux_layout<R>(n, &oi, &op, &ow, &of);
@@ -840,7 +840,6 @@ static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B,
     M25_CHECK(cudaFuncSetAttribute(k_trsv_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_bump_epoch<<<1, 1, 0, s>>>(epoch);                                    // this call's flag value
     M25_LAUNCH_CHECK("k_bump_epoch");
-    int *err = m25_dev_err_word();
     TrsvArgs<R> fa{A, lda, n, nb, inv, B, W1, nrhs, 0, flags, epoch, err};          // U^T y = b: B -> W1
     void *fargs[] = {&fa};
     M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), fargs, sm, s));
@@ -868,9 +867,11 @@ extern "C" int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void
 {
     M25_REQUIRE(d_LU && d_aux && d_B && n >= 1 && lda >= n, "m25_getrs_aux: LU, aux, B, n >= 1");
     M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs_aux: 1 to 16 right-hand sides a call");
-    return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, S(stream))
+    int *err = m25_dev_err_word();
+    return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, S(stream),
+                                          err)
                   : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)d_aux, (double *)d_B, nrhs,
-                                           S(stream));
+                                           S(stream), err);
 }
 
 extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream)
@@ -885,4 +886,19 @@ extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, i
     cudaError_t fe = cudaFreeAsync(aux, S(stream));
     if (!rc && fe != cudaSuccess) return m25_cuda_status(fe, "cudaFreeAsync");
     return rc;
+}
+
+// The solves of m25_getrs on caller-given scratch (aux_bytes >= m25_getrs_aux_bytes) with the device status word
+// err: used by m25_getrs_noalloc, whose scratch and status word are file-scope device memory.
+int m25_getrs_on_scratch(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
+                         size_t aux_bytes, int *d_err, void *d_B, int nrhs, cudaStream_t s)
+{
+    int rc = single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes, s)
+                    : getrs_prepare_impl<double>((const double *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux,
+                                                 aux_bytes, s);
+    if (rc) return rc;
+    return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, s,
+                                          d_err)
+                  : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)d_aux, (double *)d_B, nrhs,
+                                           s, d_err);
 }
