@@ -182,6 +182,7 @@ def run_gpu(args, rank, world):
             X = ds.solve_direct(f, E_dev, precision='double')
         b.record(stream)
         b.synchronize()
+        step_device.X = X
         return a.elapsed_time(b), ds.last_lu_ms
 
     # warm-up (also the accuracy check: mixed vs double at one frequency)
@@ -204,11 +205,21 @@ def run_gpu(args, rank, world):
     clk.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    lat, lu_ms, iters = [], [], []
+    def cold():
+        """A sweep starts with no kept LUs and nothing learnt (the warm-up and the accuracy check above left some)."""
+        ds.kept, ds.reach, ds.t_iter, ds.mixed_failed = [], float(np.log(2.0)), None, 0.0
+
+    cold()
+    lat, lu_ms, iters, paths, kept_X = [], [], [], {}, []
     ds.timings = {}
     for i in range(args.steps):
         ms, lms = step_device(mine[i % len(mine)], 'mixed')
-        lat.append(ms); lu_ms.append(lms); iters.append(max(ds.iters) if ds.iters else 0)
+        lat.append(ms); iters.append(max(ds.iters) if ds.iters else 0)
+        if lms is not None:
+            lu_ms.append(lms)
+        paths[ds.last_path] = paths.get(ds.last_path, 0) + 1
+        if i < args.fp64_steps:
+            kept_X.append(step_device.X)        # compared with the FP64 solve of the same frequency below
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()
@@ -220,9 +231,15 @@ def run_gpu(args, rank, world):
     for i in range(args.fp64_steps):
         ms, lms = step_device(mine[i % len(mine)], 'double')
         lat64.append(ms); lu64.append(lms)
+        if i < len(kept_X):
+            S_m = geo.sparams_from_currents(kept_X[i].cpu().numpy())
+            S_d = geo.sparams_from_currents(step_device.X.cpu().numpy())
+            dS = max(dS, float(np.abs(S_m - S_d).max()))
+    kept_X.clear()
     # end to end through the public API: E from pinned host memory, the port currents back, S on the host
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cold()
     e0.record(stream)
     for i in range(args.steps):
         sim.sparams(mine[i % len(mine)])
@@ -240,8 +257,8 @@ def run_gpu(args, rank, world):
     except Exception:
         pass
     tensor_peak = peaks.get('bf16_tflops_sustained', 1400.0)
-    lu_avg = statistics.mean(lu_ms) / 1000.0
-    achieved = flops_lu / lu_avg / 1e12
+    lu_avg = statistics.mean(lu_ms) / 1000.0 if lu_ms else float('nan')
+    achieved = flops_lu / lu_avg / 1e12 if lu_ms else 0.0
     value = world * args.steps / t_dev
     e2e = world * args.steps / t_e2e
     fp64 = (world * args.fp64_steps / t64) if args.fp64_steps else None
@@ -263,7 +280,8 @@ def run_gpu(args, rank, world):
                  "lu_ms": round(statistics.mean(lu64), 3) if lu64 else None},
         "mixed_over_fp64": round(value / fp64, 3) if fp64 else None,
         "max_dS_mixed_vs_fp64": dS, "mixed_rel_residual": res_m, "gmres_iters_max": int(max(iters)),
-        "lu_ms": round(1000 * lu_avg, 3), "phases_ms_per_step": phases,
+        "lu_ms": round(1000 * lu_avg, 3) if lu_ms else None, "factorisations": len(lu_ms), "paths": paths,
+        "phases_ms_per_step": phases,
         "e2e": {"value": round(e2e, 4), "unit": "freq-solves/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},
         "gpu_launches": int(launches),

@@ -169,6 +169,64 @@ __global__ void k_border_bottom(const double *B, const double *C, int Ne, int Nv
     }
 }
 
+// Y (n x k) = Z (n x n, row-major, leading dimension ld) X (n x k), complex128, k <= KMAX: the dense double-precision
+// product of the refinement when the double Z is resident (fast.py:1009 _solve_kept, A = Z @ V). Streams Z once
+// (HBM-bound). A block takes 8 warps x RW rows; X is staged in shared memory a chunk of JC rows at a time, column-
+// major (conflict-free reads), and every X value loaded from shared memory serves the warp's RW rows.
+template <int KMAX, int RW>
+__global__ void __launch_bounds__(256) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
+                                                      const double *__restrict__ X, int k, double *__restrict__ Y)
+{
+    constexpr int JC = 128;
+    __shared__ double2 xs[KMAX * JC];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long row0 = ((long)blockIdx.x * 8 + warp) * RW;
+    double2 acc[RW][KMAX];
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) acc[r][c] = make_double2(0.0, 0.0);
+    const double2 *Z2 = reinterpret_cast<const double2 *>(Z);
+    const double2 *X2 = reinterpret_cast<const double2 *>(X);
+    for (int j0 = 0; j0 < n; j0 += JC) {
+        const int jn = min(JC, n - j0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < JC * k; e += blockDim.x) {
+            const int j = e / k, c = e - j * k;
+            xs[c * JC + j] = j < jn ? X2[(size_t)(j0 + j) * k + c] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < JC / 32; ++q) {
+            const int jj = q * 32 + lane;
+            double2 z[RW];
+#pragma unroll
+            for (int r = 0; r < RW; ++r)
+                z[r] = (jj < jn && row0 + r < n) ? __ldcs(Z2 + (size_t)(row0 + r) * ld + j0 + jj) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int c = 0; c < KMAX; ++c) {
+                if (c < k) {
+                    const double2 x = xs[c * JC + jj];
+#pragma unroll
+                    for (int r = 0; r < RW; ++r) {
+                        acc[r][c].x = fma(z[r].x, x.x, fma(-z[r].y, x.y, acc[r][c].x));
+                        acc[r][c].y = fma(z[r].x, x.y, fma(z[r].y, x.x, acc[r][c].y));
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int c = 0; c < KMAX; ++c) {
+            double a = acc[r][c].x, b = acc[r][c].y;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); b += __shfl_xor_sync(0xffffffffu, b, o); }
+            if (lane == c && c < k && row0 + r < n) reinterpret_cast<double2 *>(Y)[(size_t)(row0 + r) * k + c] = make_double2(a, b);
+        }
+}
+
 // ======================================================================================================================
 extern "C" int m25_dotc_cols(const double *d_V, const double *d_W, long N, int k, double *d_out, void *stream)
 {
@@ -243,5 +301,23 @@ extern "C" int m25_border_mv(const double *d_B, const double *d_C, int Ne, int N
     M25_LAUNCH_CHECK("k_border_top");
     k_border_bottom<<<Nv * k, 256, 0, S(stream)>>>(d_B, d_C, Ne, Nv, d_X, k, d_Y);
     M25_LAUNCH_CHECK("k_border_bottom");
+    return M25_OK;
+}
+
+extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double *d_X, int k, double *d_Y, void *stream)
+{
+    M25_REQUIRE(d_Z && d_X && d_Y && n >= 0 && ld >= n, "m25_zgemm_skinny: Z, X, Y, ld >= n");
+    M25_REQUIRE(k >= 1 && k <= 16, "m25_zgemm_skinny: 1 to 16 columns");
+    if (!n) return M25_OK;
+    if (k <= 2) {
+        k_zgemm_skinny<2, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
+    } else if (k <= 4) {
+        k_zgemm_skinny<4, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
+    } else if (k <= 8) {
+        k_zgemm_skinny<8, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
+    } else {
+        k_zgemm_skinny<16, 2><<<(unsigned)((n + 15) / 16), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
+    }
+    M25_LAUNCH_CHECK("k_zgemm_skinny");
     return M25_OK;
 }

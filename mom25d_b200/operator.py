@@ -5,11 +5,18 @@ FastOperator.solve_direct (mom25d fast.py:704-850) behind the same call, solve_d
   precision='double'  complex128 Green tables, fill, near correction and via border into a device Z; symmetric
                       equilibration; complex128 LU with partial pivoting; the triangular solves. Matches the
                       reference's complex128 fill and LAPACK solve.
-  precision='mixed'   complex64 fill from complex64 tables, the near field's double-precision triplets added; LU in
-                      complex64 (trailing updates 3xTF32 on the tensor cores when tf32=True); refined by batched
-                      GMRES (fast.py:1437-1500) on the EXACT double-precision operator applied without a matrix:
-                      the triangle-aggregated far field (matvec_far_multi), the near field's triplets and the via
-                      border (fast.py:571-593). The refinement's residuals and corrections are double precision.
+  precision='mixed'   where the device holds a double Z and complex64 copies (24 N^2 bytes, the reference's hybrid
+                      path, fast.py:996-1084 _solve_kept): Z filled in double and equilibrated; GMRES with the dense
+                      double Z (one HBM-bound product a step) preconditioned by a complex64 LU kept from a nearby
+                      frequency (up to REUSE_KEEP of them, reach learnt as the reference does), else by a fresh
+                      complex64 LU of Z's copy (trailing updates 3xTF32 on the tensor cores when tf32=True), kept;
+                      where that does not converge, the double LU of the same Z (no second fill), and double up to
+                      MIXED_RETRY x f.
+                      Otherwise (memory): complex64 fill from complex64 tables, the near field's double-precision
+                      triplets added; complex64 LU; refined by batched GMRES (fast.py:1437-1500) on the EXACT double-
+                      precision operator applied without a matrix: the triangle-aggregated far field
+                      (matvec_far_multi), the near field's triplets and the via border (fast.py:571-593).
+                      Either way the refinement's residuals and corrections are double precision.
 
 Every step runs in libmom25d_b200 kernels; the host runs the GMRES recurrences on k x restart scalars.
 """
@@ -28,6 +35,9 @@ MIXED_MAX_ITER = 30          # fast.py:255
 FRESH_STALL = (4, 0.1)       # fast.py:256
 MIXED_RTOL = 1e-6            # fast.py:366 (FastOperator.mixed_tol)
 PREDICT_AFTER = 6            # iterations after which a fresh factor's refinement may be judged hopeless (gmres_batched)
+MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
+REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
+REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most
 
 
 class SolveFailed(RuntimeError):
@@ -45,6 +55,14 @@ class DirectSolver:
         self.timings = {}
         self.iters = []
         self._work = {}
+        self.kept = []                     # (f, factor record, dsc, seconds the fresh solve took): _solve_kept
+        self.reach = float(np.log(2.0))    # fast.py:862: |ln(f / f0)| within which a kept LU is tried
+        self.t_iter = None
+        self.mixed_failed = 0.0
+        self.reuse = True
+        self.hybrid = 'auto'               # 'auto' (when the double Z fits), True, False
+        self.last_path = None
+        self.last_lu_ms = None
 
     # ---- buffers kept across frequencies ---------------------------------------------------------------------------
     def _buf(self, name, shape, dtype):
@@ -198,6 +216,12 @@ class DirectSolver:
         E = torch.as_tensor(np.asarray(E) if not torch.is_tensor(E) else E, dtype=torch.complex128).to('cuda')
         E = E.reshape(N, -1).contiguous()
         self.iters = []
+        self.last_lu_ms = None
+        if precision == 'mixed' and f <= MIXED_RETRY * self.mixed_failed:
+            precision = 'double'                          # fast.py:740: near a failure, double
+        if precision == 'mixed' and self._hybrid_fits():
+            return self._solve_kept(f, E)
+        self.last_path = precision
         single = precision == 'mixed'
         t0 = time.perf_counter()
         Z = self.impedance(f, precision)
@@ -234,9 +258,158 @@ class DirectSolver:
             raise SolveFailed(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e})")
         return self._scale(Y, rows=dsc)
 
-    def refine(self, A, B, M, restart, maxiter, stall=None):
+    # ---- mixed precision with a resident double Z and kept complex64 LUs (fast.py:996-1118) ------------------------
+    def _hybrid_fits(self):
+        """Room for the double Z, a complex64 copy to factor and the workspaces (fast.py:720-728, on the device)."""
+        if self.hybrid != 'auto':
+            return bool(self.hybrid)
+        N = self.geo.N
+        free, _ = torch.cuda.mem_get_info()
+        held = sum(t.numel() * t.element_size() for t in self._work.values())
+        return 24.0 * N * N + 1e9 <= 0.8 * (free + held)
+
+    def _keep_max(self):
+        """LUs that may stay resident (fast.py:959-960): REUSE_KEEP, memory allowing (8 N^2 bytes each)."""
+        if not self.reuse:
+            return 0
+        N = self.geo.N
+        free, _ = torch.cuda.mem_get_info()
+        kept = sum(k[1]['bytes'] for k in self.kept)
+        return int(min(REUSE_KEEP, (0.9 * (free + kept) - 0.4e9) // (8.0 * N * N)))
+
+    def _reusable(self, f):
+        """fast.py:974-980: the kept LU nearest in frequency, if within the reach."""
+        if not self.reuse or not self.kept:
+            return None
+        k = min(self.kept, key=lambda k: abs(np.log(f / k[0])))
+        return k if abs(np.log(f / k[0])) <= self.reach else None
+
+    def _drop_kept(self):
+        """fast.py:982-987: drop the kept LU nearest another kept one."""
+        lf = np.log([k[0] for k in self.kept])
+        gap = [min((abs(lf[i] - y) for j, y in enumerate(lf) if j != i), default=0.0) for i in range(len(lf))]
+        del self.kept[int(np.argmin(gap))]
+
+    def _reach_learn(self, d, ok, iters, cap):
+        """fast.py:989-994."""
+        if ok and max(iters) <= cap // 2:
+            self.reach = max(self.reach, 1.25 * d)
+        elif not ok:
+            self.reach = min(self.reach, 0.8 * d)
+
+    def _factor_c64(self, Z64):
+        """A complex64 LU of its own (kept across frequencies): the factor in Z64's memory, pivots, the solves'
+        prepared diagonal-block inverses."""
+        N = self.geo.N
+        rec = dict(Z=Z64, ipiv=torch.empty(N, dtype=torch.int32, device='cuda'))
+        work = self._getrf_work(N, True)
+        st = self.stream if self.stream is not None else torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        check(lib().m25_getrf(P(Z64), c_long(N), c_int(N), P(rec['ipiv']), c_int(1), c_int(int(self.tf32)), P(work),
+                              ctypes.c_size_t(work.numel()), self.s), 'm25_getrf')
+        b.record(st)
+        _lib.sync_check(self.stream, 'm25_getrf')
+        self.last_lu_ms = a.elapsed_time(b)
+        nbytes = int(lib().m25_getrs_aux_bytes(c_int(N), c_int(1)))
+        rec['aux'] = torch.empty(nbytes, dtype=torch.uint8, device='cuda')
+        check(lib().m25_getrs_prepare(P(Z64), c_long(N), c_int(N), P(rec['ipiv']), c_int(1), P(rec['aux']),
+                                      ctypes.c_size_t(nbytes), self.s), 'm25_getrs_prepare')
+        rec['bytes'] = Z64.numel() * 8 + nbytes
+        return rec
+
+    def _solve_c64(self, rec, R):
+        """Z^-1 R with a kept complex64 factor, R complex128 (N x k) -> complex128."""
+        N, k = R.shape
+        R64 = torch.empty((N, k), dtype=torch.complex64, device='cuda')
+        check(lib().m25_convert(P(R), c_int(0), P(R64), c_long(N * k), self.s), 'm25_convert')
+        check(lib().m25_getrs_aux(P(rec['Z']), c_long(N), c_int(N), c_int(1), P(rec['aux']), P(R64), c_int(k), self.s),
+              'm25_getrs_aux')
+        X = torch.empty((N, k), dtype=torch.complex128, device='cuda')
+        check(lib().m25_convert(P(R64), c_int(1), P(X), c_long(N * k), self.s), 'm25_convert')
+        return X
+
+    def _dense(self, Z, V):
+        """Z V for the resident double Z (row-major N x N) and V (N x k), k <= 16 a call."""
+        N, k = V.shape
+        V = V.contiguous()
+        Y = torch.empty_like(V)
+        for c0 in range(0, k, 16):
+            c1 = min(k, c0 + 16)
+            Vc = V[:, c0:c1].contiguous() if (c0, c1) != (0, k) else V
+            Yc = torch.empty_like(Vc)
+            check(lib().m25_zgemm_skinny(P(Z), c_long(N), c_int(N), P(Vc), c_int(c1 - c0), P(Yc), self.s),
+                  'm25_zgemm_skinny')
+            Y[:, c0:c1] = Yc
+        return Y
+
+    def _solve_kept(self, f, E):
+        """fast.py:996-1084 on the device: returns the currents (equilibration undone)."""
+        geo, N = self.geo, self.geo.N
+        t0 = time.perf_counter()
+        Z = self.impedance(f, 'double')
+        self._t('fill', t0)
+        dsc = self._buf('dsc', (N,), torch.float64)
+        check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
+        dsc = dsc.clone()
+        B = self._scale(E, rows=dsc)
+        A = lambda V: self._timed('refine_matvec', lambda: self._dense(Z, V))
+        k = self._reusable(f)
+        if k is not None:
+            f0, rec, d0, t_fresh = k
+            r = (d0 / dsc).contiguous()                   # Zs^-1 ~ (D0 / D) Z0s^-1 (D0 / D)
+            cap = int(np.clip(0.8 * t_fresh / max(self.t_iter or 1e-3, 1e-6), *REUSE_ITER))
+            M = lambda R: self._timed('refine_precond', lambda: self._scale(self._solve_c64(rec, self._scale(R, rows=r)),
+                                                                              rows=r))
+            t = time.perf_counter()
+            Y, ok, rel = self.refine(A, B, M, cap, 1)
+            self.t_iter = (time.perf_counter() - t) / max(1, max(self.iters, default=1))
+            self._reach_learn(abs(np.log(f / f0)), ok, self.iters, cap)
+            if ok:
+                self.last_path = 'reused'
+                self._t('refine', t)
+                return self._scale(Y, rows=dsc)
+        t_fresh0 = time.perf_counter()
+        keep_max = self._keep_max()
+        while self.kept and len(self.kept) >= max(1, keep_max):
+            self._drop_kept()                             # room for the new factor
+        Z64 = torch.empty((N, N), dtype=torch.complex64, device='cuda')
+        check(lib().m25_convert(P(Z), c_int(0), P(Z64), c_long(N * N), self.s), 'm25_convert')
+        t = time.perf_counter()
+        rec = self._factor_c64(Z64)
+        self._t('lu', t)
+        M = lambda R: self._timed('refine_precond', lambda: self._solve_c64(rec, R))
+        t = time.perf_counter()
+        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, 1, FRESH_STALL, predict=False)
+        self.t_iter = (time.perf_counter() - t) / max(1, max(self.iters, default=1))
+        self._t('refine', t)
+        if ok:
+            self.last_path = 'fresh'
+            if keep_max >= 1:
+                self.kept.append((f, rec, dsc, time.perf_counter() - t_fresh0))
+            return self._scale(Y, rows=dsc)
+        del rec, Z64
+        # the double LU of the same (equilibrated) Z, and double up to MIXED_RETRY x f (fast.py:1074-1084)
+        self.mixed_failed = max(self.mixed_failed, f)
+        self.log.append(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e}): double LU of the "
+                        f"same Z, double up to {MIXED_RETRY * f / 1e9:.4g} GHz")
+        self.last_path = 'double (after mixed)'
+        t = time.perf_counter()
+        ipiv = self._factor(Z, False)
+        self._t('lu', t)
+        X = self._lu_solve(Z, ipiv, B, False)
+        return self._scale(X, rows=dsc)
+
+    def _timed(self, name, fn):
+        t = time.perf_counter()
+        out = fn()
+        self._t(name, t)
+        return out
+
+    def refine(self, A, B, M, restart, maxiter, stall=None, predict=True):
         """fast.py:658-663: batched GMRES to MIXED_RTOL; (Y, converged, largest relative residual)."""
-        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, maxiter=maxiter, stall=stall)
+        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, maxiter=maxiter, stall=stall,
+                                           predict=predict)
         R = B - A(Y)
         rn = np.sqrt(np.abs(self._dotc(R, R)))
         bn = np.sqrt(np.abs(self._dotc(B, B)))
@@ -244,7 +417,7 @@ class DirectSolver:
         self.residual = rel
         return Y, bool(np.isfinite(rel).all() and (rel <= 100 * MIXED_RTOL).all()), float(rel.max())
 
-    def gmres_batched(self, A, B, M=None, rtol=1e-6, restart=30, maxiter=10, stall=None):
+    def gmres_batched(self, A, B, M=None, rtol=1e-6, restart=30, maxiter=10, stall=None, predict=True):
         """fast.py:1437-1500 on device vectors: right-preconditioned restarted GMRES for k systems in lockstep,
         modified Gram-Schmidt, conjugated Givens rotations, the stall rule. The (restart x restart) Hessenberg
         recurrences run on the host."""
@@ -302,7 +475,7 @@ class DirectSolver:
                 if stall is not None and j + 1 >= stall[0] and (np.abs(g[j + 1])[live] > stall[1] * bn[act][live]).any():
                     last[live], stalled = j, True
                     break
-                if stall is not None and j + 1 >= PREDICT_AFTER:
+                if stall is not None and predict and j + 1 >= PREDICT_AFTER:
                     # the residual's geometric rate so far, extrapolated to the last iteration: a column that would
                     # still be 10x above the tolerance there ends the refinement now (its iterations would be lost:
                     # the caller solves in double precision either way)

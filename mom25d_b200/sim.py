@@ -68,7 +68,6 @@ class Simulation:
             tf32 = umma_available()
         self.fast = DirectSolver(self.geo, tf32=tf32)
         self.solver = 'direct'
-        self._mixed_failed = 0.0
         self.log.record('setup', time.perf_counter() - t, f"N={self.N}, {self.fast.dg.npairs} near pairs")
 
     @classmethod
@@ -88,16 +87,19 @@ class Simulation:
 
     def _currents(self, f, E):
         prec = self.precision
-        if prec == 'mixed' and f <= MIXED_RETRY * self._mixed_failed:
-            prec = 'double'
         t = time.perf_counter()
         try:
             I = self.fast.solve_direct(f, E, precision=prec)
         except SolveFailed as e:
+            # the matrix-free mixed path (no room for a double Z): redone in double, and up to MIXED_RETRY x f
             self.log.note(f"WARNING {e} - solving in double precision up to {MIXED_RETRY * f / 1e9:.4g} GHz")
-            self._mixed_failed = max(self._mixed_failed, f)
+            self.fast.mixed_failed = max(self.fast.mixed_failed, f)
             I = self.fast.solve_direct(f, E, precision='double')
-        self.log.record('solve', time.perf_counter() - t, f"{f / 1e9:.4g} GHz, {prec}, iters {self.fast.iters}")
+        for msg in self.fast.log:
+            self.log.note(msg)
+        self.fast.log.clear()
+        self.log.record('solve', time.perf_counter() - t, f"{f / 1e9:.4g} GHz, {self.fast.last_path}, "
+                                                          f"iters {self.fast.iters}")
         return I
 
     def port_rows(self):

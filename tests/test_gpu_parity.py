@@ -169,6 +169,51 @@ def test_mixed_solve_matches_the_reference(small, golden):
     assert max(ds.iters) <= 30
 
 
+def test_mixed_matrix_free_path_matches_the_reference(golden):
+    """The mixed path without a resident double Z (complex64 fill, matrix-free double refinement operator)."""
+    from mom25d_b200 import geometry as G
+    from mom25d_b200.operator import DirectSolver
+    geo = G.Geometry(_small_board())
+    ds = DirectSolver(geo)
+    ds.hybrid = False
+    f = float(golden['board_f'][0])
+    S = geo.sparams_from_currents(ds.solve_direct(f, geo.excitation(), precision='mixed').cpu().numpy())
+    assert ds.last_path == 'mixed'
+    assert np.abs(S - golden['board_S_double']).max() <= 1e-5
+
+
+def test_mixed_with_a_kept_lu_matches_the_reference(golden):
+    """A complex64 LU factored at 0.9 f preconditions the solve at f (fast.py:996-1084): no new factorisation,
+    the same S to the mixed bar."""
+    from mom25d_b200 import geometry as G
+    from mom25d_b200.operator import DirectSolver
+    geo = G.Geometry(_small_board())
+    ds = DirectSolver(geo)
+    f = float(golden['board_f'][0])
+    ds.solve_direct(0.9 * f, geo.excitation(), precision='mixed')
+    assert ds.last_path == 'fresh' and len(ds.kept) == 1
+    X = ds.solve_direct(f, geo.excitation(), precision='mixed').cpu().numpy()
+    assert ds.last_path == 'reused' and ds.last_lu_ms is None
+    S = geo.sparams_from_currents(X)
+    assert np.abs(S - golden['board_S_double']).max() <= 1e-5
+
+
+@pytest.mark.parametrize('k', [1, 3, 8, 11, 16])
+def test_dense_double_product(k):
+    """The refinement's dense product Y = Z X (row-major Z, N x k X) against NumPy, ragged sizes."""
+    from mom25d_b200 import _lib
+    rng = np.random.default_rng(k)
+    n = 1000 + 37 * k
+    Z = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    X = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
+    Zd, Xd = _lib.dev(Z), _lib.dev(X)
+    Yd = torch.empty_like(Xd)
+    _lib.check(_lib.lib().m25_zgemm_skinny(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(Xd), k, _lib.P(Yd),
+                                           _lib.stream_ptr()))
+    ref = Z @ X
+    assert np.abs(Yd.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize('single', [0, 1])
 @pytest.mark.parametrize('n', [300, 1000])
 def test_lu_matches_lapack(single, n):
