@@ -13,6 +13,7 @@
 //   4. trailing    A22 -= L21 U12: the complex SIMT GEMM below (FP64 / FP32), or the tensor-core 3xTF32 product
 //                  (umma.cu) for complex64 with tf32 on.
 #include <cooperative_groups.h>
+#include <type_traits>
 #include "common.cuh"
 
 static inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
@@ -621,6 +622,230 @@ __global__ void __launch_bounds__(256) k_trsv_persistent(TrsvArgs<R> a)
     }
 }
 
+// The complex64 triangular solve with the factor streamed through shared memory. Same ownership, flags and order
+// as k_trsv_persistent; what changes is how the work between two flags is done:
+//   - the factor tile of my rows x a block's columns is copied into shared memory by cp.async one task ahead (the
+//     copy of the next block's tile runs while this one waits for its flag and computes);
+//   - the apply T[r] -= A[r, b] y_b and the block solve y_b = W_b t_b are one shared-memory product (tile_mul):
+//     TPR threads a row split the columns (k mod TPR), the KR right-hand sides a compile-time count (the padding
+//     columns stay zero), y read as 16-byte pairs;
+//   - the inverses of my blocks are staged transposed, both at the start where a CTA owns two blocks;
+//   - a block is published by one fence of one thread after the CTA's barrier.
+// A task is (block, up to TRSV_RT rows); a CTA owns at most TRSV_MAXPER blocks.
+#define TRSV_RT 128
+#define TRSV_TBP (TB + 2)          // tile / inverse row stride in elements: 528 bytes, a multiple of 16
+#define TRSV_YS 18                 // y row stride: 144 bytes (16-byte aligned rows)
+#define TRSV_TS 18                 // running right-hand sides' row stride (144 bytes: conflict-free 16-byte reads)
+#define TRSV_MAXPER 5
+#define TRSV_NT 256
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+static size_t trsv_pipe_smem(int per)
+{
+    typedef cpx<float> C;
+    const int nw = per <= 2 ? per : 1;
+    return sizeof(C) * (2 * (size_t)TRSV_RT * TRSV_TBP + (size_t)nw * TB * TRSV_TBP + TB * TRSV_YS +
+                        (size_t)per * TB * TRSV_TS);
+}
+
+// out[r][c] (-)= sum_{k < kdim} M[r][k] X[k][c] for r < nrows (<= NT / TPR), c < KR; M rows of stride TRSV_TBP,
+// X rows of stride xs (16-byte aligned), out rows of stride os. All threads of the CTA call it.
+template <int KR, int TPR, bool SUB>
+__device__ __forceinline__ void tile_mul(const cpx<float> *M, int nrows, int kdim, const cpx<float> *X, int xs,
+                                         cpx<float> *out, int os)
+{
+    typedef cpx<float> C;
+    const int r = threadIdx.x / TPR, h = threadIdx.x % TPR;
+    C acc[KR];
+#pragma unroll
+    for (int c = 0; c < KR; ++c) acc[c] = mk<float>(0, 0);
+    if (r < nrows) {
+        const C *row = M + (size_t)r * TRSV_TBP;
+#pragma unroll 2
+        for (int k = h; k < kdim; k += TPR) {
+            const C v = row[k];
+            const float4 *x = reinterpret_cast<const float4 *>(X + (size_t)k * xs);
+#pragma unroll
+            for (int c2 = 0; c2 < (KR + 1) / 2; ++c2) {
+                const float4 y = x[c2];
+                cfma<float>(acc[2 * c2], v, mk<float>(y.x, y.y));
+                if (2 * c2 + 1 < KR) cfma<float>(acc[2 * c2 + 1], v, mk<float>(y.z, y.w));
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < KR; ++c)
+#pragma unroll
+        for (int o = 1; o < TPR; o <<= 1) {
+            acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
+            acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
+        }
+    if (r < nrows && h == 0) {
+#pragma unroll
+        for (int c = 0; c < KR; ++c) {
+            if (SUB) out[(size_t)r * os + c] -= acc[c];
+            else out[(size_t)r * os + c] = acc[c];
+        }
+    }
+}
+
+template <int KR>
+__global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int vec16)
+{
+    typedef cpx<float> C;
+    extern __shared__ __align__(16) unsigned char tq_raw[];
+    const int G = gridDim.x, g = blockIdx.x, nb = a.nb, nrhs = a.nrhs, n = a.n;
+    const int epoch = *(volatile const int *)a.epoch_ptr;
+    const int per = (nb + G - 1) / G, bb0 = g * per, bb1 = min(nb, bb0 + per);
+    const int R0 = bb0 * TB, R1 = min(n, bb1 * TB), nr = max(0, R1 - R0);
+    const int nw = per <= 2 ? per : 1;                                      // inverse buffers
+    C *tile = reinterpret_cast<C *>(tq_raw);                                // [2][TRSV_RT][TRSV_TBP]
+    C *Wt = tile + 2 * TRSV_RT * TRSV_TBP;                                  // [nw][TB][TRSV_TBP], transposed
+    C *Yb = Wt + (size_t)nw * TB * TRSV_TBP;                                // [TB][TRSV_YS]
+    C *T = Yb + TB * TRSV_YS;                                               // [per * TB][TRSV_TS]
+    __shared__ int ok;
+    if (nr == 0) return;
+    for (int e = threadIdx.x; e < nr * TRSV_TS; e += blockDim.x) {
+        const int r = e / TRSV_TS, c = e % TRSV_TS;
+        T[e] = c < nrhs ? ldc<float>(a.Tin, (size_t)(R0 + r) * nrhs + c) : mk<float>(0, 0);
+    }
+    for (int e = threadIdx.x; e < TB * TRSV_YS; e += blockDim.x) Yb[e] = mk<float>(0, 0);
+    if (threadIdx.x == 0) ok = 1;
+    const C *Ac = reinterpret_cast<const C *>(a.A);
+    auto blk = [&](int st) { return a.backward ? nb - 1 - st : st; };
+    const int s_last = a.backward ? nb - 1 - bb0 : bb1 - 1;
+    auto rows_of = [&](int b, int &ra, int &rb) {
+        if (b >= bb0 && b < bb1) {
+            const int b0 = b * TB, bs = min(TB, n - b0);
+            if (a.backward) { ra = R0; rb = b0; } else { ra = b0 + bs; rb = R1; }
+        } else { ra = R0; rb = R1; }
+    };
+    // ---- the tile copies, one task ahead --------------------------------------------------------------------------
+    int ls = 0, lc = 0, issued = 0;
+    auto issue_next = [&]() {
+        int ra = 0, rb = 0;
+        while (ls <= s_last) {
+            rows_of(blk(ls), ra, rb);
+            const int nch = rb > ra ? (rb - ra + TRSV_RT - 1) / TRSV_RT : 0;
+            if (lc < nch) break;
+            ++ls; lc = 0;
+        }
+        if (ls <= s_last) {
+            const int b = blk(ls), b0 = b * TB, bs = min(TB, n - b0);
+            const int r0 = ra + lc * TRSV_RT, r1 = min(rb, r0 + TRSV_RT);
+            C *dst = tile + (size_t)(issued & 1) * TRSV_RT * TRSV_TBP;
+            if (vec16) {                                                    // a warp a row: lane q copies 16 bytes
+                const int q = threadIdx.x & 31;                             // (an odd last column alone, 8 bytes)
+                if (2 * q < bs)
+                    for (int r = threadIdx.x >> 5; r < r1 - r0; r += TRSV_NT / 32) {
+                        const C *src = Ac + (size_t)(r0 + r) * a.lda + b0 + 2 * q;
+                        if (2 * q + 1 < bs) cp_async16(dst + (size_t)r * TRSV_TBP + 2 * q, src);
+                        else cp_async8(dst + (size_t)r * TRSV_TBP + 2 * q, src);
+                    }
+            } else {                                                        // 8 bytes a column: 64 threads a row
+                const int q = threadIdx.x & 63;
+                if (q < bs)
+                    for (int r = threadIdx.x >> 6; r < r1 - r0; r += TRSV_NT / 64)
+                        cp_async8(dst + (size_t)r * TRSV_TBP + q, Ac + (size_t)(r0 + r) * a.lda + b0 + q);
+            }
+            ++issued;
+            ++lc;
+        }
+        cp_async_commit();                                                  // (an empty group past the last task)
+    };
+    // block b's inverse, transposed: Wt[rr][k] = W_b[k][rr] (W_b row-major TB x TB; 16-byte loads, one round trip)
+    auto stage_w = [&](int b, C *dst) {
+        const float4 *W = reinterpret_cast<const float4 *>(
+            a.inv + 2 * ((size_t)b * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB)));
+        float4 v[TB * TB / 2 / TRSV_NT];
+#pragma unroll
+        for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) v[i] = __ldg(W + threadIdx.x + TRSV_NT * i);
+#pragma unroll
+        for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) {
+            const int e = 2 * (threadIdx.x + TRSV_NT * i), k = e / TB, rr = e % TB;   // (k, rr), (k, rr + 1)
+            dst[(size_t)rr * TRSV_TBP + k] = mk<float>(v[i].x, v[i].y);
+            dst[(size_t)(rr + 1) * TRSV_TBP + k] = mk<float>(v[i].z, v[i].w);
+        }
+    };
+    auto wbuf = [&](int b) { return Wt + (size_t)(nw == 1 ? 0 : b - bb0) * TB * TRSV_TBP; };
+    if (nw == 1) stage_w(a.backward ? bb1 - 1 : bb0, Wt);                  // my first block's inverse
+    else for (int b = bb0; b < bb1; ++b) stage_w(b, wbuf(b));               // both of mine
+    issue_next();                                                           // task 0
+    __syncthreads();
+    int used = 0;
+    for (int st = 0; st <= s_last; ++st) {
+        const int b = blk(st), b0 = b * TB, bs = min(TB, n - b0);
+        const bool mine = b >= bb0 && b < bb1;
+        if (!mine) {
+            if (threadIdx.x == 0) {
+                long it = 0;
+                while (ld_acquire_u32((const unsigned *)(a.flags + b)) != (unsigned)epoch) {
+                    if ((++it & 1023) == 0 && (it > (1L << 21) || *(volatile int *)a.err)) {   // ~1 s
+                        ok = 0; dev_error(a.err, M25_DEV_TIMEOUT); break;
+                    }
+                }
+            }
+            __syncthreads();
+            if (!ok) { cp_async_wait0(); return; }
+            {                                                               // another CTA's values: past L1,
+                const float *p = a.Xout + 2 * (size_t)b0 * nrhs;            // all loads before the stores
+                float2 v[TB * 16 / TRSV_NT];
+#pragma unroll
+                for (int i = 0; i < TB * 16 / TRSV_NT; ++i) {
+                    const int e = threadIdx.x + TRSV_NT * i;
+                    v[i] = e < bs * nrhs ? __ldcg(reinterpret_cast<const float2 *>(p) + e) : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int i = 0; i < TB * 16 / TRSV_NT; ++i) {
+                    const int e = threadIdx.x + TRSV_NT * i;
+                    if (e < bs * nrhs) Yb[(e / nrhs) * TRSV_YS + e % nrhs] = mk<float>(v[i].x, v[i].y);
+                }
+            }
+        } else {
+            // every earlier block has been applied to this block's rows: y_b = W_b^T t_b
+            tile_mul<KR, TRSV_NT / TB, false>(wbuf(b), bs, bs, T + (size_t)(b0 - R0) * TRSV_TS, TRSV_TS, Yb,
+                                              TRSV_YS);
+            __syncthreads();
+            for (int e = threadIdx.x; e < bs * nrhs; e += blockDim.x)
+                stc<float>(a.Xout, (size_t)b0 * nrhs + e, Yb[(e / nrhs) * TRSV_YS + e % nrhs]);
+            __syncthreads();
+            if (threadIdx.x == 0) {                                         // the CTA's stores, then the flag
+                __threadfence();
+                atomicExch(a.flags + b, epoch);
+            }
+            const int nxt = a.backward ? b - 1 : b + 1;                    // my next block's inverse (one buffer)
+            if (nw == 1 && nxt >= bb0 && nxt < bb1) stage_w(nxt, Wt);
+        }
+        int ra, rb;
+        rows_of(b, ra, rb);
+        for (int r0 = ra; r0 < rb; r0 += TRSV_RT) {
+            issue_next();                                                   // the next task's tile, other buffer
+            cp_async_wait1();                                               // this task's tile has landed
+            __syncthreads();
+            tile_mul<KR, TRSV_NT / TRSV_RT, true>(tile + (size_t)(used & 1) * TRSV_RT * TRSV_TBP,
+                                                  min(rb, r0 + TRSV_RT) - r0, bs, Yb, TRSV_YS,
+                                                  T + (size_t)(r0 - R0) * TRSV_TS, TRSV_TS);
+            ++used;
+            __syncthreads();                                                // the buffer is the next copy's
+        }
+        __syncthreads();
+    }
+    cp_async_wait0();
+}
+
 // X = P z: the interchanges applied from the last to the first (zlaswp with incx = -1): a permutation built in
 // shared memory by one thread, then the rows gathered
 __global__ void k_perm_from_ipiv(const int *ipiv, int n, int *perm)
@@ -841,13 +1066,31 @@ static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B,
     k_bump_epoch<<<1, 1, 0, s>>>(epoch);                                    // this call's flag value
     M25_LAUNCH_CHECK("k_bump_epoch");
     TrsvArgs<R> fa{A, lda, n, nb, inv, B, W1, nrhs, 0, flags, epoch, err};          // U^T y = b: B -> W1
-    void *fargs[] = {&fa};
-    M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), fargs, sm, s));
-    m25_note_launch();
     TrsvArgs<R> ba{A, lda, n, nb, inv, W1, W2, nrhs, 1, flags + nb, epoch, err};    // L^T z = y: W1 -> W2
-    void *bargs[] = {&ba};
-    M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), bargs, sm, s));
-    m25_note_launch();
+    const int per = (nb + G - 1) / G;
+    if (std::is_same<R, float>::value && per <= TRSV_MAXPER) {
+        // complex64: the factor tiles through shared memory (cp.async, 16-byte pieces where rows allow); the
+        // kernel for the smallest compile-time column count >= nrhs
+        const size_t psm = trsv_pipe_smem(per);
+        int vec16 = (lda % 2 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
+        const void *kf = nrhs <= 1 ? (const void *)k_trsv_pipe<1> : nrhs <= 2 ? (const void *)k_trsv_pipe<2> :
+                         nrhs <= 4 ? (const void *)k_trsv_pipe<4> : nrhs <= 8 ? (const void *)k_trsv_pipe<8> :
+                         (const void *)k_trsv_pipe<16>;
+        M25_CHECK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+        void *fargs[] = {&fa, &vec16};
+        M25_CHECK(cudaLaunchCooperativeKernel(kf, dim3(G), dim3(TRSV_NT), fargs, psm, s));
+        m25_note_launch();
+        void *bargs[] = {&ba, &vec16};
+        M25_CHECK(cudaLaunchCooperativeKernel(kf, dim3(G), dim3(TRSV_NT), bargs, psm, s));
+        m25_note_launch();
+    } else {
+        void *fargs[] = {&fa};
+        M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), fargs, sm, s));
+        m25_note_launch();
+        void *bargs[] = {&ba};
+        M25_CHECK(cudaLaunchCooperativeKernel((void *)k_trsv_persistent<R>, dim3(G), dim3(256), bargs, sm, s));
+        m25_note_launch();
+    }
     long tot = (long)n * nrhs;                                              // X = P z
     k_gather_rows<R><<<(tot + 255) / 256, 256, 0, s>>>(W2, B, perm, n, nrhs);
     M25_LAUNCH_CHECK("k_gather_rows");

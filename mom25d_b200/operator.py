@@ -63,6 +63,7 @@ class DirectSolver:
         self.hybrid = 'auto'               # 'auto' (when the double Z fits), True, False
         self.last_path = None
         self.last_lu_ms = None
+        self.attempts = []                 # reused-LU attempts: (f, f0, cap, iterations, converged, residual)
 
     # ---- buffers kept across frequencies ---------------------------------------------------------------------------
     def _buf(self, name, shape, dtype):
@@ -365,6 +366,7 @@ class DirectSolver:
             Y, ok, rel = self.refine(A, B, M, cap, 1)
             self.t_iter = (time.perf_counter() - t) / max(1, max(self.iters, default=1))
             self._reach_learn(abs(np.log(f / f0)), ok, self.iters, cap)
+            self.attempts.append(dict(f=f, f0=f0, cap=cap, iters=max(self.iters, default=0), ok=ok, rel=rel))
             if ok:
                 self.last_path = 'reused'
                 self._t('refine', t)

@@ -285,3 +285,29 @@ def test_lu_with_tensor_core_updates(n):
     Rd = _lib.dev(R.astype(np.complex64))
     _lib.check(_lib.lib().m25_getrs(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), 1, _lib.P(Rd), 2, _lib.stream_ptr()))
     assert np.abs(Rd.cpu().numpy() - x).max() < 1e-4 * np.abs(x).max()
+
+
+@pytest.mark.parametrize('n,nrhs', [(9509, 3), (9600, 8), (19000, 16)])
+def test_complex64_solves_over_several_blocks_a_cta(n, nrhs):
+    """The complex64 solves where every CTA owns two or more 64-row blocks, odd and even n (16- and 8-byte
+    copies of the factor tiles), 3 to 16 right-hand sides: against cuSOLVER's complex128 solve of the same Z."""
+    from mom25d_b200 import _lib
+    g = torch.Generator(device='cuda').manual_seed(n)
+    Z = torch.complex(torch.randn(n, n, generator=g, device='cuda'), torch.randn(n, n, generator=g, device='cuda'))
+    Z.diagonal().add_(4 * n ** 0.5)
+    R = torch.complex(torch.randn(n, nrhs, generator=g, device='cuda'), torch.randn(n, nrhs, generator=g,
+                                                                                     device='cuda'))
+    x = torch.linalg.solve(Z.to(torch.complex128), R.to(torch.complex128))
+    F = Z.clone()
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(_lib.lib().m25_getrf_workspace(n, 1))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    _lib.check(_lib.lib().m25_getrf(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 1, 1, _lib.P(work),
+                                    ctypes.c_size_t(nb), _lib.stream_ptr()))
+    for _ in range(2):                                               # twice: the flags' epochs
+        X = R.clone()
+        _lib.check(_lib.lib().m25_getrs(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 1, _lib.P(X), nrhs,
+                                        _lib.stream_ptr()))
+        _lib.sync_check()
+        err = (X.to(torch.complex128) - x).abs().max().item() / x.abs().max().item()
+        assert err < 1e-4, err
