@@ -111,20 +111,20 @@ __device__ __forceinline__ bool grid_sync(GridBarrier b, unsigned nblocks, unsig
     __syncthreads();
     if (threadIdx.x == 0) {
         ok = 1;
-        __threadfence();
+        __threadfence();                                  // release: the CTA's writes (ordered by the barrier above)
         unsigned target = phase + 1;
         if (atomicAdd(b.count, 1u) == nblocks * target - 1) {
-            __threadfence();
+            __threadfence();                              // the last arrival: everyone's writes, then the release
             atomicExch(b.gen, target);
         } else {
-            long it = 0;
+            long it = 0;                                  // acquire spin; the limit and the error word every 1024
             while (ld_acquire_u32(b.gen) < target) {
-                if (++it > (1L << 26)) { ok = 0; dev_error(err, M25_DEV_TIMEOUT); break; }
-                if (err && *(volatile int *)err) { ok = 0; break; }
-                __nanosleep(20);
+                if ((++it & 1023) == 0) {
+                    if (it > (1L << 22)) { ok = 0; dev_error(err, M25_DEV_TIMEOUT); break; }
+                    if (err && *(volatile int *)err) { ok = 0; break; }
+                }
             }
         }
-        __threadfence();
     }
     __syncthreads();
     phase += 1;

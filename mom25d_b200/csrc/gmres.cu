@@ -173,12 +173,21 @@ __global__ void k_border_bottom(const double *B, const double *C, int Ne, int Nv
 // product of the refinement when the double Z is resident (fast.py:1009 _solve_kept, A = Z @ V). Streams Z once
 // (HBM-bound). A block takes 8 warps x RW rows; X is staged in shared memory a chunk of JC rows at a time, column-
 // major (conflict-free reads), and every X value loaded from shared memory serves the warp's RW rows.
-template <int KMAX, int RW>
-__global__ void __launch_bounds__(256) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
-                                                      const double *__restrict__ X, int k, double *__restrict__ Y)
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
 {
-    constexpr int JC = 128;
-    __shared__ double2 xs[KMAX * JC];
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0) : "memory");
+}
+
+template <int KMAX>
+constexpr int zgemm_jc() { return KMAX >= 16 ? 128 : 256; }
+
+template <int KMAX, int RW>
+__global__ void __launch_bounds__(256, 2) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
+                                                         const double *__restrict__ X, int k, double *__restrict__ Y)
+{
+    constexpr int JC = zgemm_jc<KMAX>();
+    extern __shared__ __align__(16) double2 xs_dyn[];                  // [2][KMAX * JC], column-major chunks
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long row0 = ((long)blockIdx.x * 8 + warp) * RW;
     double2 acc[RW][KMAX];
@@ -188,15 +197,26 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(const double *__restrict__
         for (int c = 0; c < KMAX; ++c) acc[r][c] = make_double2(0.0, 0.0);
     const double2 *Z2 = reinterpret_cast<const double2 *>(Z);
     const double2 *X2 = reinterpret_cast<const double2 *>(X);
-    for (int j0 = 0; j0 < n; j0 += JC) {
-        const int jn = min(JC, n - j0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < JC * k; e += blockDim.x) {
-            const int j = e / k, c = e - j * k;
-            xs[c * JC + j] = j < jn ? X2[(size_t)(j0 + j) * k + c] : make_double2(0.0, 0.0);
+    // X chunk j0 .. j0 + JC into buffer buf by cp.async (zero past n and past k columns)
+    auto stage = [&](int buf, int j0) {
+        double2 *dst = xs_dyn + (size_t)buf * KMAX * JC;
+        for (int e = threadIdx.x; e < JC * KMAX; e += 256) {
+            const int j = e / KMAX, c = e % KMAX;
+            const bool ok = c < k && j0 + j < n;
+            cp_async16_zfill(dst + c * JC + j, X2 + (ok ? (size_t)(j0 + j) * k + c : 0), ok);
         }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    stage(0, 0);
+    int it = 0;
+    for (int j0 = 0; j0 < n; j0 += JC, ++it) {
+        const int jn = min(JC, n - j0);
+        if (j0 + JC < n) stage((it + 1) & 1, j0 + JC);                   // the next chunk, other buffer
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");            // this chunk has landed
         __syncthreads();
-#pragma unroll
+        const double2 *xs = xs_dyn + (size_t)(it & 1) * KMAX * JC;
+#pragma unroll 4
         for (int q = 0; q < JC / 32; ++q) {
             const int jj = q * 32 + lane;
             double2 z[RW];
@@ -204,18 +224,18 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(const double *__restrict__
             for (int r = 0; r < RW; ++r)
                 z[r] = (jj < jn && row0 + r < n) ? __ldcs(Z2 + (size_t)(row0 + r) * ld + j0 + jj) : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int c = 0; c < KMAX; ++c) {
-                if (c < k) {
-                    const double2 x = xs[c * JC + jj];
+            for (int c = 0; c < KMAX; ++c) {                                // (columns past k are zero in xs)
+                const double2 x = xs[c * JC + jj];
 #pragma unroll
-                    for (int r = 0; r < RW; ++r) {
-                        acc[r][c].x = fma(z[r].x, x.x, fma(-z[r].y, x.y, acc[r][c].x));
-                        acc[r][c].y = fma(z[r].x, x.y, fma(z[r].y, x.x, acc[r][c].y));
-                    }
+                for (int r = 0; r < RW; ++r) {
+                    acc[r][c].x = fma(z[r].x, x.x, fma(-z[r].y, x.y, acc[r][c].x));
+                    acc[r][c].y = fma(z[r].x, x.y, fma(z[r].y, x.x, acc[r][c].y));
                 }
             }
         }
+        __syncthreads();                                                 // the buffer is the chunk after next's
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
     for (int r = 0; r < RW; ++r)
 #pragma unroll
@@ -225,6 +245,16 @@ __global__ void __launch_bounds__(256) k_zgemm_skinny(const double *__restrict__
             for (int o = 16; o; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); b += __shfl_xor_sync(0xffffffffu, b, o); }
             if (lane == c && c < k && row0 + r < n) reinterpret_cast<double2 *>(Y)[(size_t)(row0 + r) * k + c] = make_double2(a, b);
         }
+}
+
+template <int KMAX, int RW>
+static int zgemm_launch(const double *d_Z, long ld, int n, const double *d_X, int k, double *d_Y, cudaStream_t s)
+{
+    const int smem = (int)(2 * sizeof(double2) * KMAX * zgemm_jc<KMAX>());
+    if (smem > 48 * 1024) M25_CHECK(cudaFuncSetAttribute(k_zgemm_skinny<KMAX, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_zgemm_skinny<KMAX, RW><<<(unsigned)((n + 8 * RW - 1) / (8 * RW)), 256, smem, s>>>(d_Z, ld, n, d_X, k, d_Y);
+    M25_LAUNCH_CHECK("k_zgemm_skinny");
+    return M25_OK;
 }
 
 // ======================================================================================================================
@@ -309,15 +339,9 @@ extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double 
     M25_REQUIRE(d_Z && d_X && d_Y && n >= 0 && ld >= n, "m25_zgemm_skinny: Z, X, Y, ld >= n");
     M25_REQUIRE(k >= 1 && k <= 16, "m25_zgemm_skinny: 1 to 16 columns");
     if (!n) return M25_OK;
-    if (k <= 2) {
-        k_zgemm_skinny<2, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
-    } else if (k <= 4) {
-        k_zgemm_skinny<4, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
-    } else if (k <= 8) {
-        k_zgemm_skinny<8, 4><<<(unsigned)((n + 31) / 32), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
-    } else {
-        k_zgemm_skinny<16, 2><<<(unsigned)((n + 15) / 16), 256, 0, S(stream)>>>(d_Z, ld, n, d_X, k, d_Y);
-    }
-    M25_LAUNCH_CHECK("k_zgemm_skinny");
-    return M25_OK;
+    // fewer rows a warp as the columns grow (registers: two CTAs an SM keep enough loads of Z in flight)
+    if (k <= 2) return zgemm_launch<2, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    if (k <= 4) return zgemm_launch<4, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    return zgemm_launch<16, 1>(d_Z, ld, n, d_X, k, d_Y, S(stream));
 }

@@ -113,11 +113,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         __syncthreads();
         const int wb = si[0], p = s_p;
         if (wb < 0) { dev_error(err, M25_DEV_INDEX); return; }
-        if (tid < jb) {
-            const volatile R *cu = (const volatile R *)(cand_row + ((size_t)par * G + wb) * NB + tid);
-            const volatile R *cd = (const volatile R *)(drow + par * NB + tid);
-            U[tid] = mk<R>(cu[0], cu[1]);
-            D[tid] = mk<R>(cd[0], cd[1]);
+        if (tid < jb) {                                             // other CTAs' rows: past L1, one load each
+            typedef typename vec2_of<R>::type V2;
+            const V2 u = __ldcg(reinterpret_cast<const V2 *>(cand_row + ((size_t)par * G + wb) * NB + tid));
+            const V2 d = __ldcg(reinterpret_cast<const V2 *>(drow + par * NB + tid));
+            U[tid] = mk<R>(u.x, u.y);
+            D[tid] = mk<R>(d.x, d.y);
         }
         __syncthreads();
         if (tid < jb) {
@@ -223,11 +224,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(R *A, long lda, int n, 
         __syncthreads();
         const int wb = si[0], p = s_p;
         if (wb < 0) { dev_error(err, M25_DEV_INDEX); return; }
-        if (tid < jb) {           // other blocks' writes: read past L1
-            const volatile R *cu = (const volatile R *)(cand_row + ((size_t)par * G + wb) * NB + tid);
-            const volatile R *cd = (const volatile R *)(drow + par * NB + tid);
-            U[tid] = mk<R>(cu[0], cu[1]);
-            D[tid] = mk<R>(cd[0], cd[1]);
+        if (tid < jb) {           // other blocks' writes: read past L1, one load each
+            typedef typename vec2_of<R>::type V2;
+            const V2 u = __ldcg(reinterpret_cast<const V2 *>(cand_row + ((size_t)par * G + wb) * NB + tid));
+            const V2 d = __ldcg(reinterpret_cast<const V2 *>(drow + par * NB + tid));
+            U[tid] = mk<R>(u.x, u.y);
+            D[tid] = mk<R>(d.x, d.y);
         }
         __syncthreads();
         // 4. the interchange, by the owners of the two rows
@@ -377,6 +379,121 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
             size_t o = (size_t)nn * lda + m;
             stc<R>(Cm, o, ldc<R>(Cm, o) - acc[i][j]);
         }
+    }
+}
+
+// The complex128 update C -= A B on the FP64 tensor cores (mma.sync m8n8k4 f64; Blackwell's tcgen05 has no FP64
+// kind). Column-major A (M x K), B (K x N), C (M x N), one leading dimension. A 64 x 64 tile a CTA of four warps, each
+// warp 32 x 32 complex: 4 x 4 tiles of 8 x 8 for the real and the imaginary part, C_re -= A_re B_re - A_im B_im,
+// C_im -= A_re B_im + A_im B_re (four real products). K in slices of 16 staged in shared memory as separate real
+// and imaginary planes (strides chosen so that the fragment loads are conflict-free), the next slice prefetched in
+// registers.
+#define ZD_BM 64
+#define ZD_BN 64
+#define ZD_BK 16
+#define ZD_SA (ZD_BM + 8)          // A planes: [k][m], m contiguous
+#define ZD_SB (ZD_BK + 4)          // B planes: [n][k], k contiguous
+
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8_zfill(void *smem, const void *gmem, bool valid)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+
+static size_t zdmma_smem() { return sizeof(double) * 2 * 2 * ((size_t)ZD_BK * ZD_SA + (size_t)ZD_BN * ZD_SB); }
+
+__global__ void __launch_bounds__(128, 2) k_zgemm_dmma(double *Cm, const double *Am, const double *Bm, long lda, int M,
+                                                       int N, int K)
+{
+    extern __shared__ __align__(16) double zd_raw[];
+    typedef double APlane[ZD_BK][ZD_SA];
+    typedef double BPlane[ZD_BN][ZD_SB];
+    APlane *As = reinterpret_cast<APlane *>(zd_raw);                          // [buf * 2 + re / im]
+    BPlane *Bs = reinterpret_cast<BPlane *>(zd_raw + 4 * ZD_BK * ZD_SA);      // [buf * 2 + re / im]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m0 = blockIdx.y * ZD_BM, n0 = blockIdx.x * ZD_BN;
+    const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+    double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+    // a K slice into buffer buf: 8-byte asynchronous copies that split the complex numbers into the two planes
+    auto stage = [&](int buf, int kk) {
+        for (int e = tid; e < ZD_BM * ZD_BK; e += 128) {
+            const int k = e / ZD_BM, m = e % ZD_BM;                               // A: m fastest (contiguous)
+            const bool ok = m0 + m < M && kk + k < K;
+            const double *src = Am + 2 * (ok ? (size_t)(kk + k) * lda + m0 + m : 0);
+            cp_async8_zfill(&As[2 * buf][k][m], src, ok);
+            cp_async8_zfill(&As[2 * buf + 1][k][m], src + 1, ok);
+        }
+        for (int e = tid; e < ZD_BN * ZD_BK; e += 128) {
+            const int nn = e / ZD_BK, k = e % ZD_BK;                              // B: k fastest (contiguous)
+            const bool ok = n0 + nn < N && kk + k < K;
+            const double *src = Bm + 2 * (ok ? (size_t)(n0 + nn) * lda + kk + k : 0);
+            cp_async8_zfill(&Bs[2 * buf][nn][k], src, ok);
+            cp_async8_zfill(&Bs[2 * buf + 1][nn][k], src + 1, ok);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    stage(0, 0);
+    int buf = 0;
+    const int fr = lane >> 2, fk = lane & 3;       // fragment coordinates: A row / B column, k
+    for (int kk = 0; kk < K; kk += ZD_BK) {
+        if (kk + ZD_BK < K) stage(buf ^ 1, kk + ZD_BK);                           // the next slice, other buffer
+        else asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < ZD_BK; k4 += 4) {
+            double ar[4], ai[4], br[4], bi[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ar[i] = As[2 * buf][k4 + fk][wm + 8 * i + fr];
+                ai[i] = As[2 * buf + 1][k4 + fk][wm + 8 * i + fr];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                br[j] = Bs[2 * buf][wn + 8 * j + fr][k4 + fk];
+                bi[j] = Bs[2 * buf + 1][wn + 8 * j + fr][k4 + fk];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dmma_8x8x4(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+                    dmma_8x8x4(cr[i][j][0], cr[i][j][1], -ai[i], bi[j]);
+                    dmma_8x8x4(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+                    dmma_8x8x4(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                }
+        }
+        __syncthreads();                                                          // the buffer is the next stage's
+        buf ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // C -= the product: this lane's accumulators are rows fr, columns 2 fk, 2 fk + 1 of each 8 x 8 tile
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + wm + 8 * i + fr;
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int nn = n0 + wn + 8 * j + 2 * fk + h;
+                if (nn >= N) continue;
+                double2 *p = reinterpret_cast<double2 *>(Cm) + (size_t)nn * lda + m;
+                double2 c = *p;
+                c.x -= cr[i][j][h];
+                c.y -= ci[i][j][h];
+                *p = c;
+            }
     }
 }
 
@@ -930,6 +1047,7 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     int nb2 = NB2;                                                   // outer panel (M25_NB2: tuning, a multiple of NB)
     if (const char *e = getenv("M25_NB2")) nb2 = std::max(NB, atoi(e) / NB * NB);
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
+    M25_CHECK(cudaFuncSetAttribute(k_zgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdmma_smem()));
     auto laswp = [&](int r0, int nsw, long c0, long c1) -> int {
         if (c1 <= c0) return M25_OK;
         k_laswp<R><<<(c1 - c0 + 127) / 128, 128, 0, s>>>(A, lda, n, r0, nsw, ipiv, c0, c1);
@@ -951,6 +1069,13 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
         if (sizeof(R) == 4 && tf32 && big)
             return m25_umma_trailing((float *)C22, lda, M, Nc, K, (const float *)L21, (const float *)U12, umma_work,
                                      umma_bytes, s);
+        if (sizeof(R) == 8) {                                      // complex128: the FP64 tensor cores
+            dim3 grid((Nc + ZD_BN - 1) / ZD_BN, (M + ZD_BM - 1) / ZD_BM);
+            k_zgemm_dmma<<<grid, 128, zdmma_smem(), s>>>((double *)C22, (const double *)L21, (const double *)U12, lda,
+                                                         M, Nc, K);
+            M25_LAUNCH_CHECK("k_zgemm_dmma");
+            return M25_OK;
+        }
         dim3 grid((Nc + 63) / 64, (M + 127) / 128);
         k_gemm_update<R><<<grid, 256, gemm_smem<R>(), s>>>(C22, L21, U12, lda, M, Nc, K);
         M25_LAUNCH_CHECK("k_gemm_update");

@@ -2,7 +2,9 @@
 mom25d_b200.tune - timings of the hot path's kernels on this GPU, and the choice of their tile parameters.
 
     python -m mom25d_b200.tune --lu 8192 [--single] [--tf32] [--reps 3]     # the LU alone, CUDA events
-    python -m mom25d_b200.tune --fill                                        # fill / near / tables, 20k board
+    python -m mom25d_b200.tune --update 4096 4096 256                        # the tensor-core trailing update
+    python -m mom25d_b200.tune --solve 18788 [--single]                      # the triangular solves, 8 columns
+    python -m mom25d_b200.tune --dense 18788 8                               # the dense double product
 
 Times are CUDA-event measurements on the launching stream after a warm-up, the matrix a random complex one with a
 dominant diagonal (pivots away from it as well).
@@ -106,10 +108,30 @@ def time_solve(n, nrhs=8, single=True, reps=5):
     return dict(n=n, nrhs=nrhs, single=single, ms=ms, factor_GBps=n * n * (8 if single else 16) / ms / 1e6)
 
 
+def time_dense(n, k=8, reps=5):
+    """The refinement's dense double product Y = Z X (m25_zgemm_skinny): HBM-bound, 16 n^2 bytes of Z a call."""
+    Z = random_matrix(n, torch.complex128)
+    X = random_matrix(max(n, k), torch.complex128, seed=3)[:n, :k].contiguous()
+    Y = torch.empty_like(X)
+    s = torch.cuda.current_stream()
+    out = []
+    for r in range(reps + 1):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        check(lib().m25_zgemm_skinny(P(Z), ctypes.c_long(n), n, P(X), k, P(Y), _lib.stream_ptr()), 'm25_zgemm_skinny')
+        b.record(s)
+        _lib.sync_check()
+        if r:
+            out.append(a.elapsed_time(b))
+    ms = float(np.median(out))
+    return dict(n=n, k=k, ms=ms, GBps=16.0 * n * n / ms / 1e6)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--update', type=int, nargs=3, default=None, metavar=('M', 'N', 'K'))
     ap.add_argument('--solve', type=int, default=0)
+    ap.add_argument('--dense', type=int, nargs=2, default=None, metavar=('N', 'K'))
     ap.add_argument('--lu', type=int, default=0)
     ap.add_argument('--single', action='store_true')
     ap.add_argument('--tf32', action='store_true')
@@ -120,6 +142,8 @@ def main():
         print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
     if a.update:
         print(json.dumps(time_update(*a.update, reps=a.reps)))
+    if a.dense:
+        print(json.dumps(time_dense(*a.dense, reps=a.reps)))
     if a.solve:
         print(json.dumps(time_solve(a.solve, single=a.single, reps=a.reps)))
 
