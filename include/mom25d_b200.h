@@ -195,6 +195,11 @@ int m25_equilibrate_c64(float *d_Z, long n, long ld, double *d_dsc_out, void *st
 int m25_dotc_cols(const double *d_V, const double *d_W, long N, int k, double *d_out, void *stream);
 /* W[n, c] += V[n, c] a[c]. */
 int m25_axpy_cols(double *d_W, const double *d_V, const double *d_a, long N, int k, void *stream);
+/* The Gram-Schmidt step against a whole Krylov basis (batched GMRES, fast.py:1437-1500, as classical Gram-Schmidt
+ * applied twice): out[i, c] = sum_n conj(V_i[n, c]) W[n, c] for the nv blocks V_i (N x k each, consecutive);
+ * W -= sum_i V_i h[i, c] (h complex128[nv * k]). */
+int m25_dotc_multi(const double *d_V, int nv, long N, int k, const double *d_W, double *d_out, void *stream);
+int m25_axpy_multi(double *d_W, const double *d_V, int nv, long N, int k, const double *d_h, void *stream);
 /* Y[n, c] = X[n, c] s[c] (times rows[n] when d_rows != NULL); s complex128[k] or NULL for 1. */
 int m25_scale_cols(double *d_Y, const double *d_X, const double *d_s, const double *d_rows, long N, int k,
                    void *stream);

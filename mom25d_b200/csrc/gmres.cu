@@ -257,6 +257,46 @@ static int zgemm_launch(const double *d_Z, long ld, int n, const double *d_X, in
     return M25_OK;
 }
 
+// The Gram-Schmidt step of the batched GMRES against all basis vectors at once (classical Gram-Schmidt, applied
+// twice by the caller): out[i, c] = sum_n conj(V_i[n, c]) W[n, c] for i < nv (V: nv consecutive N x k blocks), one
+// grid row of blocks per vector; W -= sum_i V_i h[i] (h: nv x k complex, per column).
+__global__ void k_dotc_multi(const double *V, long N, int k, const double *W, double *out)
+{
+    const double *Vi = V + 2 * (size_t)blockIdx.y * N * k;
+    __shared__ double sx[16][33], sy[16][33];
+    double ax[16], ay[16];
+    for (int c = 0; c < 16; ++c) ax[c] = ay[c] = 0;
+    for (long n = blockIdx.x * (long)blockDim.x + threadIdx.x; n < N; n += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < k; ++c) {
+            zd v = ldc<double>(Vi, (size_t)n * k + c), w = ldc<double>(W, (size_t)n * k + c);
+            ax[c] += v.x * w.x + v.y * w.y;
+            ay[c] += v.x * w.y - v.y * w.x;
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int c = 0; c < k; ++c) {
+        double x = ax[c], y = ay[c];
+        for (int o = 16; o; o >>= 1) { x += __shfl_xor_sync(0xffffffffu, x, o); y += __shfl_xor_sync(0xffffffffu, y, o); }
+        if (lane == 0) { sx[c][wid] = x; sy[c][wid] = y; }
+    }
+    __syncthreads();
+    if (threadIdx.x < k) {
+        double x = 0, y = 0;
+        for (int j = 0; j < (int)(blockDim.x / 32); ++j) { x += sx[threadIdx.x][j]; y += sy[threadIdx.x][j]; }
+        atomicAdd(out + 2 * ((size_t)blockIdx.y * k + threadIdx.x), x);
+        atomicAdd(out + 2 * ((size_t)blockIdx.y * k + threadIdx.x) + 1, y);
+    }
+}
+
+__global__ void k_axpy_multi(double *W, const double *V, int nv, long N, int k, const double *h)
+{
+    long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= N * k) return;
+    const int c = e % k;
+    zd w = ldc<double>(W, e);
+    for (int i = 0; i < nv; ++i) cfms<double>(w, ldc<double>(V, (size_t)i * N * k + e), ldc<double>(h, (size_t)i * k + c));
+    stc<double>(W, e, w);
+}
+
 // ======================================================================================================================
 extern "C" int m25_dotc_cols(const double *d_V, const double *d_W, long N, int k, double *d_out, void *stream)
 {
@@ -344,4 +384,23 @@ extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double 
     if (k <= 4) return zgemm_launch<4, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     return zgemm_launch<16, 1>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+}
+
+extern "C" int m25_dotc_multi(const double *d_V, int nv, long N, int k, const double *d_W, double *d_out, void *stream)
+{
+    M25_REQUIRE(k >= 1 && k <= 16 && nv >= 1 && nv <= 65535, "m25_dotc_multi: 1 to 16 columns, nv >= 1");
+    M25_CHECK(cudaMemsetAsync(d_out, 0, sizeof(double) * 2 * (size_t)nv * k, S(stream)));
+    dim3 grid((unsigned)std::min<long>(148, (N + 255) / 256), (unsigned)nv);
+    k_dotc_multi<<<grid, 256, 0, S(stream)>>>(d_V, N, k, d_W, d_out);
+    M25_LAUNCH_CHECK("k_dotc_multi");
+    return M25_OK;
+}
+
+extern "C" int m25_axpy_multi(double *d_W, const double *d_V, int nv, long N, int k, const double *d_h, void *stream)
+{
+    long t = N * k;
+    if (!t || nv <= 0) return M25_OK;
+    k_axpy_multi<<<(t + 255) / 256, 256, 0, S(stream)>>>(d_W, d_V, nv, N, k, d_h);
+    M25_LAUNCH_CHECK("k_axpy_multi");
+    return M25_OK;
 }
