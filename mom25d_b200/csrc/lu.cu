@@ -33,6 +33,7 @@ struct PanelWork {
     double *cand_row;     // [2][G][NB] complex (as R pairs; sized for double)
     double *drow;         // [2][NB] complex
     GridBarrier bar;
+    unsigned *gen;        // [2][G]: the column (+ 1) whose candidate a CTA has published (k_panel_smem)
 };
 
 // The panel with each block's rows held in shared memory for the whole panel (Ps[c * cs + i], row r0 + i): the
@@ -51,11 +52,11 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
     const int cs = (rows + G - 1) / G;
     const int r0 = k0 + b * cs, r1 = min(n, r0 + cs);
     const int nr = max(0, r1 - r0);
-    unsigned phase = 0;
     __shared__ C U[NB], D[NB];
     __shared__ double sv[PANEL_THREADS / 32];
     __shared__ int si[PANEL_THREADS / 32];
-    __shared__ int s_p;
+    __shared__ int s_p, s_fail;
+    __shared__ int sw[PANEL_THREADS / 32];
     __shared__ C s_recip;
     C *cand_row = reinterpret_cast<C *>(pw.cand_row);
     C *drow = reinterpret_cast<C *>(pw.drow);
@@ -63,6 +64,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         int c = e / nr, i = e % nr;
         Ps[c * cs + i] = ldc<R>(A, (size_t)(k0 + c) * lda + r0 + i);
     }
+    if (tid == 0) s_fail = 0;
     __syncthreads();
     for (int j = 0; j < jb; ++j) {
         const int col = k0 + j, par = j & 1;
@@ -89,26 +91,43 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         __syncthreads();
         if (s_p != 0x7fffffff && tid < jb) cand_row[((size_t)par * G + b) * NB + tid] = Ps[tid * cs + (s_p - r0)];
         if (col >= r0 && col < r1 && tid < jb) drow[par * NB + tid] = Ps[tid * cs + (col - r0)];
-        if (!grid_sync(pw.bar, G, phase, err)) return;
-        if (tid < 32) {
-            double bv = -1.0;
-            int bw = -1, brow = 0x7fffffff;
-            for (unsigned w = tid; w < G; w += 32) {
-                double v = __ldcg(pw.cand_val + par * G + w);
-                int ri = __ldcg(pw.cand_idx + par * G + w);
-                if (ri == 0x7fffffff) continue;
-                if (v > bv || (v == bv && ri < brow)) { bv = v; bw = (int)w; brow = ri; }
+        // the exchange of this column's candidates: no counter, no second round trip. Each CTA publishes its
+        // record (candidate, its row, the diagonal row) with a per-CTA generation; thread w < G waits for CTA w's
+        // generation and reads its candidate, and the CTA reduces them itself
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(pw.gen + par * G + b, (unsigned)(j + 1));
+        }
+        double bv = -1.0;
+        int bw = -1, brow = 0x7fffffff;
+        if (tid < (int)G) {
+            long it = 0;
+            bool ok = true;
+            while (ld_acquire_u32(pw.gen + par * G + tid) != (unsigned)(j + 1)) {
+                if ((++it & 1023) == 0 && (it > (1L << 22) || *(volatile int *)err)) { ok = false; break; }
             }
-            for (int o = 16; o; o >>= 1) {
-                double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                int ow = __shfl_xor_sync(0xffffffffu, bw, o), orow = __shfl_xor_sync(0xffffffffu, brow, o);
-                if (ov > bv || (ov == bv && orow < brow)) { bv = ov; bw = ow; brow = orow; }
+            if (!ok) { s_fail = 1; dev_error(err, M25_DEV_TIMEOUT); }
+            else {
+                const double v = __ldcg(pw.cand_val + par * G + tid);
+                const int ri = __ldcg(pw.cand_idx + par * G + tid);
+                if (ri != 0x7fffffff) { bv = v; bw = tid; brow = ri; }
             }
-            if (tid == 0) {
-                si[0] = bw;
-                s_p = brow;
-                if (b == 0 && bw >= 0) ipiv[col] = brow;
-            }
+        }
+        for (int o = 16; o; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int ow = __shfl_xor_sync(0xffffffffu, bw, o), orow = __shfl_xor_sync(0xffffffffu, brow, o);
+            if (ov > bv || (ov == bv && orow < brow)) { bv = ov; bw = ow; brow = orow; }
+        }
+        if ((tid & 31) == 0) { sv[tid >> 5] = bv; si[tid >> 5] = brow; sw[tid >> 5] = bw; }
+        __syncthreads();
+        if (s_fail) return;
+        if (tid == 0) {
+            for (int w = 1; w < PANEL_THREADS / 32; ++w)
+                if (sv[w] > bv || (sv[w] == bv && si[w] < brow)) { bv = sv[w]; bw = sw[w]; brow = si[w]; }
+            si[0] = bw;
+            s_p = brow;
+            if (b == 0 && bw >= 0) ipiv[col] = brow;
         }
         __syncthreads();
         const int wb = si[0], p = s_p;
@@ -1007,7 +1026,7 @@ extern "C" size_t m25_getrf_workspace(int n, int single)
     b += 2 * (size_t)G * sizeof(int) + 256;                         // cand_idx
     b += 2 * (size_t)G * NB * 2 * sizeof(double) + 256;             // cand_row
     b += 2 * NB * 2 * sizeof(double) + 256;                         // drow
-    b += 2 * sizeof(unsigned) + 256;                                // barrier
+    b += (2 + 2 * (size_t)G) * sizeof(unsigned) + 256;             // barrier, the panel's generations
     if (single) b += m25_umma_workspace(n, NB) + 256;
     (void)n;
     return b;
@@ -1029,10 +1048,11 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     pw.cand_idx = (int *)take(2 * (size_t)G * sizeof(int));
     pw.cand_row = (double *)take(2 * (size_t)G * NB * 2 * sizeof(double));
     pw.drow = (double *)take(2 * NB * 2 * sizeof(double));
-    unsigned *bar = (unsigned *)take(2 * sizeof(unsigned));
+    unsigned *bar = (unsigned *)take((2 + 2 * (size_t)G) * sizeof(unsigned));
     void *umma_work = take(0);
     size_t umma_bytes = work_bytes - ((unsigned char *)umma_work - (unsigned char *)work);
     pw.bar.count = bar; pw.bar.gen = bar + 1;
+    pw.gen = bar + 2;
     int *err = m25_dev_err_word();
     M25_CHECK(cudaMemsetAsync(ipiv, 0xff, sizeof(int) * (size_t)n, s));      // -1 until the panel sets it
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
@@ -1092,7 +1112,7 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             int Gp = std::min(gmax, std::max(1, (n - k0 + 31) / 32));
             const int cs = (n - k0 + Gp - 1) / Gp;
             const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
-            M25_CHECK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+            M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), s));
             void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
             if (psmem <= (size_t)smem_cap)
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R>, dim3(Gp), dim3(PANEL_THREADS), args,
@@ -1103,14 +1123,14 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             if ((rc = laswp(k0, jb, 0, k0))) return rc;                    // left: the factored L columns
             if ((rc = laswp(k0, jb, k0 + jb, KE))) return rc;              // the rest of the outer panel
             if ((rc = trsm(k0, jb, k0 + jb, KE))) return rc;
-            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, false))) return rc;
+            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, true))) return rc;
         }
         if (KE < n) {
             if ((rc = laswp(K0, JB, KE, n))) return rc;                    // the outer panel's interchanges, right
             for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
                 const int jb = std::min(NB, KE - k0);
                 if ((rc = trsm(k0, jb, KE, n))) return rc;
-                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, false))) return rc;
+                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, true))) return rc;
             }
             if ((rc = gemm(KE, n - KE, KE, n - KE, K0, JB, true))) return rc;   // the trailing update, depth nb2
         }
