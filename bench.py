@@ -183,7 +183,7 @@ def run_gpu(args, rank, world):
         b.record(stream)
         b.synchronize()
         step_device.X = X
-        return a.elapsed_time(b), ds.last_lu_ms
+        return a.elapsed_time(b), (ds.last_lu_c64_ms if precision == 'mixed' else ds.last_lu_ms)
 
     # warm-up (also the accuracy check: mixed vs double at one frequency)
     for i in range(args.warmup):
@@ -264,9 +264,11 @@ def run_gpu(args, rank, world):
     fp64 = (world * args.fp64_steps / t64) if args.fp64_steps else None
     bytes_h2d = int(E_host.numel() * 16)
     bytes_d2h = int(len(sim.port_rows()[0]) * E_host.shape[1] * 16)
-    traffic = None
+    traffic = None                           # DRAM bytes of one complex64 factorisation, from an ncu capture
     try:
-        traffic = json.load(open(os.path.join(ROOT, 'profiles', 'traffic.json'))).get('lu_trailing_update')
+        cap = json.load(open(os.path.join(ROOT, 'profiles', 'traffic.json')))['complex64_lu']
+        if int(cap['n']) == N:
+            traffic = cap['bytes_per_factorisation']
     except Exception:
         pass
     line = {
@@ -285,7 +287,7 @@ def run_gpu(args, rank, world):
         "e2e": {"value": round(e2e, 4), "unit": "freq-solves/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "complex LU (m25_getrf: panel + trailing update), 8/3 N^3 flops a factorisation",
+        "roofline": {"kernel": "complex64 LU with 3xTF32 tcgen05 updates (m25_getrf), 8/3 N^3 flops a factorisation",
                      "bound": "tensor", "achieved": round(achieved, 2), "peak": tensor_peak, "unit": "TFLOP/s",
                      "frac": round(achieved / tensor_peak, 4), "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else "fallback"},

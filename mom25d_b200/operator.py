@@ -62,7 +62,7 @@ class DirectSolver:
         self.reuse = True
         self.hybrid = 'auto'               # 'auto' (when the double Z fits), True, False
         self.last_path = None
-        self.last_lu_ms = None
+        self.last_lu_ms = self.last_lu_c64_ms = None
         self.attempts = []                 # reused-LU attempts: (f, f0, cap, iterations, converged, residual)
 
     # ---- buffers kept across frequencies ---------------------------------------------------------------------------
@@ -230,7 +230,7 @@ class DirectSolver:
         E = torch.as_tensor(np.asarray(E) if not torch.is_tensor(E) else E, dtype=torch.complex128).to('cuda')
         E = E.reshape(N, -1).contiguous()
         self.iters = []
-        self.last_lu_ms = None
+        self.last_lu_ms = self.last_lu_c64_ms = None
         if precision == 'mixed' and f <= MIXED_RETRY * self.mixed_failed:
             precision = 'double'                          # fast.py:740: near a failure, double
         if precision == 'mixed' and self._hybrid_fits():
@@ -324,7 +324,7 @@ class DirectSolver:
                               ctypes.c_size_t(work.numel()), self.s), 'm25_getrf')
         b.record(st)
         _lib.sync_check(self.stream, 'm25_getrf')
-        self.last_lu_ms = a.elapsed_time(b)
+        self.last_lu_ms = self.last_lu_c64_ms = a.elapsed_time(b)
         nbytes = int(lib().m25_getrs_aux_bytes(c_int(N), c_int(1)))
         rec['aux'] = torch.empty(nbytes, dtype=torch.uint8, device='cuda')
         check(lib().m25_getrs_prepare(P(Z64), c_long(N), c_int(N), P(rec['ipiv']), c_int(1), P(rec['aux']),
