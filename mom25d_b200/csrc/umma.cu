@@ -203,10 +203,10 @@ __global__ void __launch_bounds__(128, 1) k_umma_update(float *C, long ldc_f, in
                 float *p = C + (size_t)(n0 + c0) * ldc_f + row;
                 const int nv = min(32, Nc - (n0 + c0));
 #pragma unroll
-                for (int j = 0; j < 32; ++j) cv[j] = j < nv ? __ldcg(p + (size_t)j * ldc_f) : 0.f;
+                for (int j = 0; j < 32; ++j) cv[j] = j < nv ? __ldcs(p + (size_t)j * ldc_f) : 0.f;
 #pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (j < nv) __stcg(p + (size_t)j * ldc_f, cv[j] - __uint_as_float(v[j]));
+                for (int j = 0; j < 32; ++j)    // (streaming: C is read and written once, the operands stay in L2)
+                    if (j < nv) __stcs(p + (size_t)j * ldc_f, cv[j] - __uint_as_float(v[j]));
             }
         }
     }

@@ -1,0 +1,240 @@
+"""
+mom25d_b200.serve - (board, frequency) solves served as they arrive, several at once on one GPU.
+
+    python -m mom25d_b200.serve [--rate 20] [--requests 40] [--slots 4] [--seed 0]
+
+The north-star serving mode of the hot path (the reference solves one board's sweep at a time, sim.py:331 /
+run.py:41; this is the request loop a service puts in front of it):
+
+  - boards stay resident: each board's mesh, near-pair lists and device geometry are built on its first request
+    and kept, one solver per (board, slot), so later requests for the board pay only the per-frequency work;
+  - continuous batching: a request is admitted as soon as it has arrived, a slot is free and its device-memory
+    footprint (the double Z, its complex64 copy and the LU workspaces: 24 N^2 bytes plus workspace) fits the
+    budget beside the requests in flight; admitted requests run concurrently, each slot on its own CUDA stream
+    and host thread (the library's calls release the interpreter lock), so their kernels overlap on the device;
+  - results do not depend on the mix: no reduction crosses requests and kept-LU reuse is off here (a reused
+    factor would make a request's iterations depend on the one before it), so a request's S is the same alone and
+    in the mix up to the rounding of the near field's atomic additions;
+  - latency is completion minus arrival; p50 / p99 and solves / s are reported.
+
+Request.S holds the scattering matrix (nports x nports complex).
+"""
+import argparse
+import heapq
+import json
+import queue
+import threading
+import time
+
+import numpy as np
+
+GB = 1e9
+
+
+class Request:
+    __slots__ = ('rid', 'board', 'f', 'arrival', 'start', 'done', 'S', 'error', 'slot', 'path', 'iters')
+
+    def __init__(self, rid, board, f, arrival=0.0):
+        self.rid, self.board, self.f, self.arrival = rid, board, float(f), float(arrival)
+        self.start = self.done = None
+        self.S = self.error = self.slot = self.path = None
+        self.iters = []
+
+    @property
+    def latency(self):
+        return None if self.done is None else self.done - self.arrival
+
+
+def footprint_bytes(N, single_workspace=None):
+    """Device memory one mixed-precision request holds while it runs (operator.DirectSolver._solve_kept): the double
+    Z (16 N^2), its complex64 copy factored in place (8 N^2), the LU and solve workspaces, the near-field lists and
+    the Krylov basis (a fixed 1 GB allowance)."""
+    ws = single_workspace if single_workspace is not None else 0
+    return 24.0 * N * N + ws + 1.0 * GB
+
+
+class Server:
+    """Serves Request objects for the boards given as {key: Board}. solve(slot, key, f) -> (S, info) can be
+    replaced (tests drive the admission logic with a stand-in on the CPU); the default solves on the GPU."""
+
+    def __init__(self, boards, slots=4, budget_bytes=None, precision='mixed', solve=None, sizes=None):
+        self.boards = dict(boards)
+        self.slots = int(slots)
+        self.precision = precision
+        self._sizes = dict(sizes or {})
+        self._geo, self._solvers, self._streams = {}, {}, {}
+        self._lock = threading.Lock()
+        self._solve = solve or self._solve_gpu
+        if budget_bytes is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info()
+            budget_bytes = 0.8 * free
+        self.budget = float(budget_bytes)
+
+    # ---- the per-board state, built on first use -----------------------------------------------------------------
+    def size(self, key):
+        if key not in self._sizes:
+            self._sizes[key] = self._geometry(key).N
+        return self._sizes[key]
+
+    def _geometry(self, key):
+        with self._lock:
+            if key not in self._geo:
+                from .geometry import Geometry
+                self._geo[key] = Geometry(self.boards[key])
+            return self._geo[key]
+
+    def _solver(self, slot, key):
+        import torch
+        from .operator import DirectSolver
+        from . import umma_available
+        if slot not in self._streams:
+            self._streams[slot] = torch.cuda.Stream()
+        if (slot, key) not in self._solvers:
+            with torch.cuda.stream(self._streams[slot]):
+                ds = DirectSolver(self._geometry(key), stream=self._streams[slot], tf32=umma_available())
+                ds.reuse = False                       # results independent of the request order
+                self._solvers[(slot, key)] = ds
+        return self._solvers[(slot, key)], self._streams[slot]
+
+    def _solve_gpu(self, slot, key, f):
+        import torch
+        ds, stream = self._solver(slot, key)
+        geo = self._geometry(key)
+        with torch.cuda.stream(stream):
+            X = ds.solve_direct(f, geo.excitation(), precision=self.precision)
+            S = geo.sparams_from_currents(X.cpu().numpy())
+            stream.synchronize()
+        return S, dict(path=ds.last_path, iters=list(ds.iters))
+
+    def footprint(self, key):
+        return footprint_bytes(self.size(key))
+
+    # ---- the loop ------------------------------------------------------------------------------------------------
+    def run(self, requests, clock=time.perf_counter):
+        """Serves the requests (arrival times in seconds from the call) and returns them completed."""
+        reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        for r in reqs:
+            if self.footprint(r.board) > self.budget:
+                raise MemoryError(f"request {r.rid}: board {r.board!r} needs {self.footprint(r.board) / GB:.1f} GB, "
+                                  f"above the serving budget of {self.budget / GB:.1f} GB")
+        t0 = clock()
+        done_q = queue.Queue()
+        work_qs = [queue.Queue() for _ in range(self.slots)]
+
+        def worker(slot):
+            while True:
+                r = work_qs[slot].get()
+                if r is None:
+                    return
+                r.start = clock() - t0
+                try:
+                    r.S, info = self._solve(slot, r.board, r.f)
+                    r.path, r.iters = info.get('path'), info.get('iters', [])
+                except Exception as e:                   # reported on the request; the loop keeps serving
+                    r.error = f"{type(e).__name__}: {e}"
+                r.done = clock() - t0
+                done_q.put((slot, r))
+
+        threads = [threading.Thread(target=worker, args=(s,), daemon=True) for s in range(self.slots)]
+        for t in threads:
+            t.start()
+        free_slots = list(range(self.slots))
+        in_flight, used = 0, 0.0
+        waiting = []                                      # arrived, not yet admitted: (arrival, rid, request)
+        i = 0
+        try:
+            while i < len(reqs) or waiting or in_flight:
+                now = clock() - t0
+                while i < len(reqs) and reqs[i].arrival <= now:
+                    heapq.heappush(waiting, (reqs[i].arrival, reqs[i].rid, reqs[i]))
+                    i += 1
+                # admit in arrival order while a slot is free and the footprint fits (first come, first served)
+                while waiting and free_slots and used + self.footprint(waiting[0][2].board) <= self.budget:
+                    _, _, r = heapq.heappop(waiting)
+                    slot = free_slots.pop(0)
+                    r.slot = slot
+                    used += self.footprint(r.board)
+                    in_flight += 1
+                    work_qs[slot].put(r)
+                timeout = None
+                if i < len(reqs):
+                    timeout = max(0.0, reqs[i].arrival - (clock() - t0))
+                if in_flight == 0 and timeout is not None:
+                    time.sleep(timeout)
+                    continue
+                try:
+                    slot, r = done_q.get(timeout=timeout if timeout is not None else 3600.0)
+                except queue.Empty:
+                    continue
+                free_slots.append(slot)
+                free_slots.sort()
+                used -= self.footprint(r.board)
+                in_flight -= 1
+        finally:
+            for q in work_qs:
+                q.put(None)
+            for t in threads:
+                t.join(timeout=60)
+        return reqs
+
+    @staticmethod
+    def report(reqs, wall):
+        lat = np.array([r.latency for r in reqs if r.error is None])
+        return dict(requests=len(reqs), errors=sum(r.error is not None for r in reqs),
+                    solves_per_s=round(len(lat) / wall, 3) if wall > 0 else None,
+                    p50_ms=round(1000 * float(np.percentile(lat, 50)), 1) if len(lat) else None,
+                    p99_ms=round(1000 * float(np.percentile(lat, 99)), 1) if len(lat) else None)
+
+
+def poisson_requests(keys, weights, rate, count, fmin=0.5e9, fmax=10e9, seed=0):
+    """Seeded Poisson arrivals at `rate` per second; board drawn with `weights`, frequency U[fmin, fmax]."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, count))
+    w = np.asarray(weights, float) / np.sum(weights)
+    boards = rng.choice(len(keys), size=count, p=w)
+    fs = rng.uniform(fmin, fmax, count)
+    return [Request(i, keys[b], fs[i], t[i]) for i, b in enumerate(boards)]
+
+
+def board_pool(seed=0, targets=(2000, 5000, 10000, 20000)):
+    """Seeded synthetic routed boards of about the given unknown counts: the 20k-unknown generator with the trace
+    count and the area scaled by N / 20000 (the unknown count follows the copper area)."""
+    from .board import routed_board
+    pool = {}
+    for j, n in enumerate(targets):
+        s = n / 20000.0
+        pool[f"routed_{n}"] = routed_board(seed=seed + j, n_traces=max(2, int(round(24 * s))),
+                                           n_vias=max(2, int(round(16 * s))), n_ports=max(2, min(8, int(round(8 * s)))),
+                                           size=(60e-3 * s ** 0.5, 40e-3 * s ** 0.5), ncross=4)
+    return pool
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--rate', type=float, default=20.0)
+    ap.add_argument('--requests', type=int, default=40)
+    ap.add_argument('--slots', type=int, default=4)
+    ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--targets', type=int, nargs='+', default=[2000, 5000, 10000, 20000])
+    ap.add_argument('--weights', type=float, nargs='+', default=None)
+    a = ap.parse_args()
+    import torch
+    torch.cuda.set_device(0)
+    pool = board_pool(a.seed, tuple(a.targets))
+    keys = list(pool)
+    weights = a.weights or [0.3, 0.3, 0.2, 0.15, 0.05][:len(keys)]
+    srv = Server(pool, slots=a.slots)
+    for k in keys:                                        # resident boards: geometry built before serving
+        srv.size(k)
+    reqs = poisson_requests(keys, weights, a.rate, a.requests, seed=a.seed)
+    t = time.perf_counter()
+    srv.run(reqs)
+    wall = time.perf_counter() - t
+    out = dict(rate=a.rate, slots=a.slots, sizes={k: srv.size(k) for k in keys}, wall_s=round(wall, 3))
+    out.update(Server.report(reqs, wall))
+    print(json.dumps(out))
+
+
+if __name__ == '__main__':
+    main()
