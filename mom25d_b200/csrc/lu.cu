@@ -402,118 +402,135 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
 }
 
 // The complex128 update C -= A B on the FP64 tensor cores (mma.sync m8n8k4 f64; Blackwell's tcgen05 has no FP64
-// kind). Column-major A (M x K), B (K x N), C (M x N), one leading dimension. A 64 x 64 tile a CTA of four warps, each
-// warp 32 x 32 complex: 4 x 4 tiles of 8 x 8 for the real and the imaginary part, C_re -= A_re B_re - A_im B_im,
-// C_im -= A_re B_im + A_im B_re (four real products). K in slices of 16 staged in shared memory as separate real
-// and imaginary planes (strides chosen so that the fragment loads are conflict-free), the next slice prefetched in
-// registers.
+// kind). Column-major A (M x K), B (K x N), C (M x N), one leading dimension. A 64 x 64 tile a CTA of four warps,
+// each warp 32 x 32 complex: 2 x 4 tiles of 16 x 8 (mma m16n8k8) for the real and the imaginary part,
+// C_re -= A_re B_re - A_im B_im, C_im -= A_re B_im + A_im B_re (four real products). K in slices of 16 copied into
+// shared memory by cp.async (double-buffered), one 16-byte copy and one 16-byte fragment read a complex number.
 #define ZD_BM 64
 #define ZD_BN 64
 #define ZD_BK 16
-#define ZD_SA (ZD_BM + 8)          // A planes: [k][m], m contiguous
-#define ZD_SB (ZD_BK + 4)          // B planes: [n][k], k contiguous
+#define ZD_SA (ZD_BM + 2)          // A slice [k][m], complex: a row stride = 2 mod 8 keeps the 16-byte reads conflict-free
+#define ZD_SB (ZD_BK + 4)          // B slice [n][k], complex: 4 mod 8
 
-__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b)
+// D (16 x 8) += A (16 x 8, row) B (8 x 8, col), FP64. Lane l = 4 g + t holds A[g][t], A[g + 8][t], A[g][t + 4],
+// A[g + 8][t + 4]; B[t][g], B[t + 4][g]; D[g][2 t], D[g][2 t + 1], D[g + 8][2 t], D[g + 8][2 t + 1].
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2])
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-__device__ __forceinline__ void cp_async8_zfill(void *smem, const void *gmem, bool valid)
+__device__ __forceinline__ void cp_async16_zfill_lu(void *smem, const void *gmem, bool valid)
 {
     unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 16 : 0) : "memory");
 }
 
-static size_t zdmma_smem() { return sizeof(double) * 2 * 2 * ((size_t)ZD_BK * ZD_SA + (size_t)ZD_BN * ZD_SB); }
+static size_t zdmma_smem() { return sizeof(double2) * 2 * ((size_t)ZD_BK * ZD_SA + (size_t)ZD_BN * ZD_SB); }
 
 __global__ void __launch_bounds__(128, 2) k_zgemm_dmma(double *Cm, const double *Am, const double *Bm, long lda, int M,
                                                        int N, int K)
 {
-    extern __shared__ __align__(16) double zd_raw[];
-    typedef double APlane[ZD_BK][ZD_SA];
-    typedef double BPlane[ZD_BN][ZD_SB];
-    APlane *As = reinterpret_cast<APlane *>(zd_raw);                          // [buf * 2 + re / im]
-    BPlane *Bs = reinterpret_cast<BPlane *>(zd_raw + 4 * ZD_BK * ZD_SA);      // [buf * 2 + re / im]
+    extern __shared__ __align__(16) double2 zd_raw[];
+    typedef double2 ASlice[ZD_BK][ZD_SA];
+    typedef double2 BSlice[ZD_BN][ZD_SB];
+    ASlice *As = reinterpret_cast<ASlice *>(zd_raw);                           // [buf]
+    BSlice *Bs = reinterpret_cast<BSlice *>(zd_raw + 2 * ZD_BK * ZD_SA);       // [buf]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int m0 = blockIdx.y * ZD_BM, n0 = blockIdx.x * ZD_BN;
     const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-    double cr[4][4][2], ci[4][4][2];
+    double cr[2][4][4], ci[2][4][4];                 // [16-row tile][8-column tile][fragment]
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
-    // a K slice into buffer buf: 8-byte asynchronous copies that split the complex numbers into the two planes
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) cr[i][j][q] = ci[i][j][q] = 0.0;
+    const double2 *A2 = reinterpret_cast<const double2 *>(Am), *B2 = reinterpret_cast<const double2 *>(Bm);
+    // a K slice into buffer buf: one 16-byte asynchronous copy a complex number
     auto stage = [&](int buf, int kk) {
         for (int e = tid; e < ZD_BM * ZD_BK; e += 128) {
             const int k = e / ZD_BM, m = e % ZD_BM;                               // A: m fastest (contiguous)
             const bool ok = m0 + m < M && kk + k < K;
-            const double *src = Am + 2 * (ok ? (size_t)(kk + k) * lda + m0 + m : 0);
-            cp_async8_zfill(&As[2 * buf][k][m], src, ok);
-            cp_async8_zfill(&As[2 * buf + 1][k][m], src + 1, ok);
+            cp_async16_zfill_lu(&As[buf][k][m], A2 + (ok ? (size_t)(kk + k) * lda + m0 + m : 0), ok);
         }
         for (int e = tid; e < ZD_BN * ZD_BK; e += 128) {
             const int nn = e / ZD_BK, k = e % ZD_BK;                              // B: k fastest (contiguous)
             const bool ok = n0 + nn < N && kk + k < K;
-            const double *src = Bm + 2 * (ok ? (size_t)(n0 + nn) * lda + kk + k : 0);
-            cp_async8_zfill(&Bs[2 * buf][nn][k], src, ok);
-            cp_async8_zfill(&Bs[2 * buf + 1][nn][k], src + 1, ok);
+            cp_async16_zfill_lu(&Bs[buf][nn][k], B2 + (ok ? (size_t)(n0 + nn) * lda + kk + k : 0), ok);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     stage(0, 0);
     int buf = 0;
-    const int fr = lane >> 2, fk = lane & 3;       // fragment coordinates: A row / B column, k
+    const int fg = lane >> 2, ft = lane & 3;       // fragment coordinates (group, thread in group)
     for (int kk = 0; kk < K; kk += ZD_BK) {
         if (kk + ZD_BK < K) stage(buf ^ 1, kk + ZD_BK);                           // the next slice, other buffer
         else asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 1;" ::: "memory");
         __syncthreads();
 #pragma unroll
-        for (int k4 = 0; k4 < ZD_BK; k4 += 4) {
-            double ar[4], ai[4], br[4], bi[4];
+        for (int k8 = 0; k8 < ZD_BK; k8 += 8) {
+            double ar[2][4], ai[2][4], nai[2][4], br[4][2], bi[4][2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                ar[i] = As[2 * buf][k4 + fk][wm + 8 * i + fr];
-                ai[i] = As[2 * buf + 1][k4 + fk][wm + 8 * i + fr];
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + 16 * i + fg;
+                const double2 v0 = As[buf][k8 + ft][r], v1 = As[buf][k8 + ft][r + 8];
+                const double2 v2 = As[buf][k8 + ft + 4][r], v3 = As[buf][k8 + ft + 4][r + 8];
+                ar[i][0] = v0.x; ai[i][0] = v0.y;
+                ar[i][1] = v1.x; ai[i][1] = v1.y;
+                ar[i][2] = v2.x; ai[i][2] = v2.y;
+                ar[i][3] = v3.x; ai[i][3] = v3.y;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) nai[i][q] = -ai[i][q];
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                br[j] = Bs[2 * buf][wn + 8 * j + fr][k4 + fk];
-                bi[j] = Bs[2 * buf + 1][wn + 8 * j + fr][k4 + fk];
+                const int c = wn + 8 * j + fg;
+                const double2 w0 = Bs[buf][c][k8 + ft], w1 = Bs[buf][c][k8 + ft + 4];
+                br[j][0] = w0.x; bi[j][0] = w0.y;
+                br[j][1] = w1.x; bi[j][1] = w1.y;
             }
+            // two passes over the 8 tiles: independent products between two into the same accumulator
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 2; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    dmma_8x8x4(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
-                    dmma_8x8x4(cr[i][j][0], cr[i][j][1], -ai[i], bi[j]);
-                    dmma_8x8x4(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
-                    dmma_8x8x4(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                    dmma_16x8x8(cr[i][j], ar[i], br[j]);
+                    dmma_16x8x8(ci[i][j], ar[i], bi[j]);
+                }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dmma_16x8x8(cr[i][j], nai[i], bi[j]);
+                    dmma_16x8x8(ci[i][j], ai[i], br[j]);
                 }
         }
         __syncthreads();                                                          // the buffer is the next stage's
         buf ^= 1;
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // C -= the product: this lane's accumulators are rows fr, columns 2 fk, 2 fk + 1 of each 8 x 8 tile
+    // C -= the product: fragment q of tile (i, j) is row g (+ 8 for q >= 2), column 2 t + (q & 1)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int m = m0 + wm + 8 * i + fr;
-        if (m >= M) continue;
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int q = 0; q < 4; ++q) {
+            const int m = m0 + wm + 16 * i + fg + (q >= 2 ? 8 : 0);
+            if (m >= M) continue;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int nn = n0 + wn + 8 * j + 2 * fk + h;
+            for (int j = 0; j < 4; ++j) {
+                const int nn = n0 + wn + 8 * j + 2 * ft + (q & 1);
                 if (nn >= N) continue;
                 double2 *p = reinterpret_cast<double2 *>(Cm) + (size_t)nn * lda + m;
                 double2 c = *p;
-                c.x -= cr[i][j][h];
-                c.y -= ci[i][j][h];
+                c.x -= cr[i][j][q];
+                c.y -= ci[i][j][q];
                 *p = c;
             }
-    }
+        }
 }
 
 template <typename R>
