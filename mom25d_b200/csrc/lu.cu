@@ -1044,10 +1044,37 @@ extern "C" size_t m25_getrf_workspace(int n, int single)
     b += 2 * (size_t)G * NB * 2 * sizeof(double) + 256;             // cand_row
     b += 2 * NB * 2 * sizeof(double) + 256;                         // drow
     b += (2 + 2 * (size_t)G) * sizeof(unsigned) + 256;             // barrier, the panel's generations
-    if (single) b += m25_umma_workspace(n, NB) + 256;
+    if (single) b += 2 * (m25_umma_workspace(n, NB) + 256);          // one a stream (look-ahead)
     (void)n;
     return b;
 }
+
+// The LU's two internal streams on the current device: a high-priority one for the panels and everything on the
+// critical path, a low-priority one for the trailing update of the previous outer block, so that the next block's
+// panels run while that update does (look-ahead); and the events between them. One set per host thread and device,
+// created on the thread's first factorisation there (calls from different threads, e.g. concurrent requests on
+// their own streams, do not share them; calls from one thread are ordered by it).
+namespace {
+struct LuStreams { cudaStream_t hi = nullptr, lo = nullptr; cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; };
+thread_local LuStreams g_lu[64];
+
+int lu_streams(LuStreams *out)
+{
+    int dev = -1;
+    M25_CHECK(cudaGetDevice(&dev));
+    M25_REQUIRE(dev >= 0 && dev < 64, "m25_getrf: device index above 63");
+    LuStreams &L = g_lu[dev];
+    if (!L.hi) {
+        int least = 0, greatest = 0;
+        M25_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        M25_CHECK(cudaStreamCreateWithPriority(&L.hi, cudaStreamNonBlocking, greatest));
+        M25_CHECK(cudaStreamCreateWithPriority(&L.lo, cudaStreamNonBlocking, least));
+        for (auto &e : L.ev) M25_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    *out = L;
+    return M25_OK;
+}
+}  // namespace
 
 template <typename R>
 static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, size_t work_bytes, cudaStream_t s)
@@ -1066,12 +1093,21 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     pw.cand_row = (double *)take(2 * (size_t)G * NB * 2 * sizeof(double));
     pw.drow = (double *)take(2 * NB * 2 * sizeof(double));
     unsigned *bar = (unsigned *)take((2 + 2 * (size_t)G) * sizeof(unsigned));
-    void *umma_work = take(0);
-    size_t umma_bytes = work_bytes - ((unsigned char *)umma_work - (unsigned char *)work);
+    void *umma_work0 = take(0);
+    size_t umma_bytes = (work_bytes - ((unsigned char *)umma_work0 - (unsigned char *)work)) / 2 / 256 * 256;
+    void *umma_work1 = (unsigned char *)umma_work0 + umma_bytes;
     pw.bar.count = bar; pw.bar.gen = bar + 1;
     pw.gen = bar + 2;
     int *err = m25_dev_err_word();
-    M25_CHECK(cudaMemsetAsync(ipiv, 0xff, sizeof(int) * (size_t)n, s));      // -1 until the panel sets it
+    LuStreams st;
+    int rc = lu_streams(&st);
+    if (rc) return rc;
+    const cudaStream_t H = st.hi, Lo = st.lo;
+    cudaEvent_t ev_start = st.ev[0], ev_p = st.ev[1], ev_u = st.ev[2], ev_end = st.ev[3];
+    M25_CHECK(cudaEventRecord(ev_start, s));                        // the caller's work first
+    M25_CHECK(cudaStreamWaitEvent(H, ev_start, 0));
+    M25_CHECK(cudaStreamWaitEvent(Lo, ev_start, 0));
+    M25_CHECK(cudaMemsetAsync(ipiv, 0xff, sizeof(int) * (size_t)n, H));      // -1 until the panel sets it
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
     M25_CHECK(cudaFuncSetAttribute(k_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
     int smem_optin = 0, dev = 0;
@@ -1085,43 +1121,46 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     if (const char *e = getenv("M25_NB2")) nb2 = std::max(NB, atoi(e) / NB * NB);
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
     M25_CHECK(cudaFuncSetAttribute(k_zgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdmma_smem()));
-    auto laswp = [&](int r0, int nsw, long c0, long c1) -> int {
+    auto laswp = [&](int r0, int nsw, long c0, long c1, cudaStream_t cs) -> int {
         if (c1 <= c0) return M25_OK;
-        k_laswp<R><<<(c1 - c0 + 127) / 128, 128, 0, s>>>(A, lda, n, r0, nsw, ipiv, c0, c1);
+        k_laswp<R><<<(c1 - c0 + 127) / 128, 128, 0, cs>>>(A, lda, n, r0, nsw, ipiv, c0, c1);
         M25_LAUNCH_CHECK("k_laswp");
         return M25_OK;
     };
-    auto trsm = [&](int k0, int jb, long c0, long c1) -> int {
+    auto trsm = [&](int k0, int jb, long c0, long c1, cudaStream_t cs) -> int {
         if (c1 <= c0) return M25_OK;
-        k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, s>>>(A, lda, k0, jb, c0, c1);
+        k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, cs>>>(A, lda, k0, jb, c0, c1);
         M25_LAUNCH_CHECK("k_trsm");
         return M25_OK;
     };
-    // C = A[r0 .., c0 ..] (M x Nc) -= A[r0 .., k0 .. k0 + K] A[k0 .. k0 + K, c0 ..]
-    auto gemm = [&](int r0, int M, long c0, int Nc, int k0, int K, bool big) -> int {
+    // C = A[r0 .., c0 ..] (M x Nc) -= A[r0 .., k0 .. k0 + K] A[k0 .. k0 + K, c0 ..]; the low-priority stream's
+    // tensor-core updates split their operands into the second workspace
+    auto gemm = [&](int r0, int M, long c0, int Nc, int k0, int K, bool big, cudaStream_t cs) -> int {
         if (M <= 0 || Nc <= 0 || K <= 0) return M25_OK;
         R *C22 = A + 2 * ((size_t)c0 * lda + r0);
         const R *L21 = A + 2 * ((size_t)k0 * lda + r0);
         const R *U12 = A + 2 * ((size_t)c0 * lda + k0);
         if (sizeof(R) == 4 && tf32 && big)
-            return m25_umma_trailing((float *)C22, lda, M, Nc, K, (const float *)L21, (const float *)U12, umma_work,
-                                     umma_bytes, s);
+            return m25_umma_trailing((float *)C22, lda, M, Nc, K, (const float *)L21, (const float *)U12,
+                                     cs == Lo ? umma_work1 : umma_work0, umma_bytes, cs);
         if (sizeof(R) == 8) {                                      // complex128: the FP64 tensor cores
             dim3 grid((Nc + ZD_BN - 1) / ZD_BN, (M + ZD_BM - 1) / ZD_BM);
-            k_zgemm_dmma<<<grid, 128, zdmma_smem(), s>>>((double *)C22, (const double *)L21, (const double *)U12, lda,
-                                                         M, Nc, K);
+            k_zgemm_dmma<<<grid, 128, zdmma_smem(), cs>>>((double *)C22, (const double *)L21, (const double *)U12,
+                                                          lda, M, Nc, K);
             M25_LAUNCH_CHECK("k_zgemm_dmma");
             return M25_OK;
         }
         dim3 grid((Nc + 63) / 64, (M + 127) / 128);
-        k_gemm_update<R><<<grid, 256, gemm_smem<R>(), s>>>(C22, L21, U12, lda, M, Nc, K);
+        k_gemm_update<R><<<grid, 256, gemm_smem<R>(), cs>>>(C22, L21, U12, lda, M, Nc, K);
         M25_LAUNCH_CHECK("k_gemm_update");
         return M25_OK;
     };
-    int rc;
     // Two levels: outer panels of nb2 columns, each factored as panels of NB (pivoting, interchanges, TRSM and
-    // updates restricted to the outer panel); then the outer panel's interchanges, TRSM and one trailing update
-    // of depth nb2 over the rest of the matrix.
+    // updates restricted to the outer panel); then the outer panel's interchanges, TRSM and the trailing update of
+    // depth nb2. Look-ahead: the update of the next outer panel's columns runs on the high-priority stream H, the
+    // update of all the columns after it on the low-priority stream Lo, while H factors the next outer panel
+    // (disjoint columns); H waits for Lo before it touches those columns (interchanges, TRSM) again.
+    bool lo_pending = false;
     for (int K0 = 0; K0 < n; K0 += nb2) {
         const int JB = std::min(nb2, n - K0), KE = K0 + JB;
         for (int k0 = K0; k0 < KE; k0 += NB) {
@@ -1129,29 +1168,44 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             int Gp = std::min(gmax, std::max(1, (n - k0 + 31) / 32));
             const int cs = (n - k0 + Gp - 1) / Gp;
             const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
-            M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), s));
+            M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), H));
             void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
             if (psmem <= (size_t)smem_cap)
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R>, dim3(Gp), dim3(PANEL_THREADS), args,
-                                                      psmem, s));
+                                                      psmem, H));
             else
-                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, s));
+                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, H));
             m25_note_launch();
-            if ((rc = laswp(k0, jb, 0, k0))) return rc;                    // left: the factored L columns
-            if ((rc = laswp(k0, jb, k0 + jb, KE))) return rc;              // the rest of the outer panel
-            if ((rc = trsm(k0, jb, k0 + jb, KE))) return rc;
-            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, true))) return rc;
+            if ((rc = laswp(k0, jb, 0, k0, H))) return rc;                 // left: the factored L columns
+            if ((rc = laswp(k0, jb, k0 + jb, KE, H))) return rc;           // the rest of the outer panel
+            if ((rc = trsm(k0, jb, k0 + jb, KE, H))) return rc;
+            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, true, H))) return rc;
         }
         if (KE < n) {
-            if ((rc = laswp(K0, JB, KE, n))) return rc;                    // the outer panel's interchanges, right
+            if (lo_pending) {                                               // the previous block's update of [KE, n)
+                M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));
+                lo_pending = false;
+            }
+            if ((rc = laswp(K0, JB, KE, n, H))) return rc;                 // the outer panel's interchanges, right
             for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
                 const int jb = std::min(NB, KE - k0);
-                if ((rc = trsm(k0, jb, KE, n))) return rc;
-                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, true))) return rc;
+                if ((rc = trsm(k0, jb, KE, n, H))) return rc;
+                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, true, H))) return rc;
             }
-            if ((rc = gemm(KE, n - KE, KE, n - KE, K0, JB, true))) return rc;   // the trailing update, depth nb2
+            const int KE2 = std::min(n, KE + nb2);                          // the next outer panel's columns
+            if ((rc = gemm(KE, n - KE, KE, KE2 - KE, K0, JB, true, H))) return rc;
+            if (KE2 < n) {                                                  // the rest, beside the next panels
+                M25_CHECK(cudaEventRecord(ev_p, H));
+                M25_CHECK(cudaStreamWaitEvent(Lo, ev_p, 0));
+                if ((rc = gemm(KE, n - KE, KE2, n - KE2, K0, JB, true, Lo))) return rc;
+                M25_CHECK(cudaEventRecord(ev_u, Lo));
+                lo_pending = true;
+            }
         }
     }
+    if (lo_pending) M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));
+    M25_CHECK(cudaEventRecord(ev_end, H));                           // the caller's stream waits for both
+    M25_CHECK(cudaStreamWaitEvent(s, ev_end, 0));
     return M25_OK;
 }
 
