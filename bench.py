@@ -211,13 +211,21 @@ def run_gpu(args, rank, world):
 
     cold()
     lat, lu_ms, iters, paths, kept_X = [], [], [], {}, []
-    ds.timings = {}
+    ds.timings, ds.attempts = {}, []
     for i in range(args.steps):
         ms, lms = step_device(mine[i % len(mine)], 'mixed')
         lat.append(ms); iters.append(max(ds.iters) if ds.iters else 0)
         if lms is not None:
             lu_ms.append(lms)
         paths[ds.last_path] = paths.get(ds.last_path, 0) + 1
+        if args.verbose:
+            print(f"step {i}: {mine[i % len(mine)] / 1e9:.4g} GHz {ds.last_path:22s} {iters[-1]:3d} iterations "
+                  f"{ms:8.1f} ms", file=sys.stderr)
+    attempts = list(ds.attempts)
+    if args.verbose:
+        for a in attempts:
+            print(f"reuse {a['f'] / 1e9:.4g} GHz from {a['f0'] / 1e9:.4g}: cap {a['cap']}, {a['iters']} iterations, "
+                  f"{'converged' if a['ok'] else 'not converged'} ({a['rel']:.1e})", file=sys.stderr)
         if i < args.fp64_steps:
             kept_X.append(step_device.X)        # compared with the FP64 solve of the same frequency below
     ev1.record(stream)
@@ -283,6 +291,7 @@ def run_gpu(args, rank, world):
         "mixed_over_fp64": round(value / fp64, 3) if fp64 else None,
         "max_dS_mixed_vs_fp64": dS, "mixed_rel_residual": res_m, "gmres_iters_max": int(max(iters)),
         "lu_ms": round(1000 * lu_avg, 3) if lu_ms else None, "factorisations": len(lu_ms), "paths": paths,
+        "reuse_attempts": {"tried": len(attempts), "converged": sum(1 for a in attempts if a['ok'])},
         "phases_ms_per_step": phases,
         "e2e": {"value": round(e2e, 4), "unit": "freq-solves/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},
@@ -330,6 +339,7 @@ def main():
     ap.add_argument('--impl', default='b200')
     ap.add_argument('--ref-lu', type=int, default=6000)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--verbose', action='store_true', help='each timed step and reuse attempt on stderr')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world = int(os.environ.get('RANK', 0)), int(os.environ.get('WORLD_SIZE', 1))

@@ -1102,7 +1102,8 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     LuStreams st;
     int rc = lu_streams(&st);
     if (rc) return rc;
-    const cudaStream_t H = st.hi, Lo = st.lo;
+    const char *la = getenv("M25_LOOKAHEAD");                       // 0: one stream (the same results, in order)
+    const cudaStream_t H = st.hi, Lo = (la && atoi(la) == 0) ? st.hi : st.lo;
     cudaEvent_t ev_start = st.ev[0], ev_p = st.ev[1], ev_u = st.ev[2], ev_end = st.ev[3];
     M25_CHECK(cudaEventRecord(ev_start, s));                        // the caller's work first
     M25_CHECK(cudaStreamWaitEvent(H, ev_start, 0));
@@ -1176,16 +1177,21 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             else
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, H));
             m25_note_launch();
-            if ((rc = laswp(k0, jb, 0, k0, H))) return rc;                 // left: the factored L columns
+            if ((rc = laswp(k0, jb, K0, k0, H))) return rc;                // left, inside the outer panel
             if ((rc = laswp(k0, jb, k0 + jb, KE, H))) return rc;           // the rest of the outer panel
             if ((rc = trsm(k0, jb, k0 + jb, KE, H))) return rc;
-            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, true, H))) return rc;
+            // in FP32 on the CUDA cores, not 3xTF32: the columns of L pass through every update of their outer
+            // panel, and the tensor-core error there (about 2^-22 a product against 2^-24) costs the factor its
+            // use as a preconditioner near the low-frequency end (fresh LUs at 0.67 and 0.91 GHz of the routed
+            // board no longer converged; the FP32 inner update costs 5 ms of 236 at N = 18,788)
+            if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, false, H))) return rc;
         }
+        if (lo_pending) {                                                   // the previous block's update of [KE, n)
+            M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));                     // reads L of the earlier columns: their
+            lo_pending = false;                                             // interchanges wait for it
+        }
+        if ((rc = laswp(K0, JB, 0, K0, H))) return rc;                     // the outer panel's interchanges, left
         if (KE < n) {
-            if (lo_pending) {                                               // the previous block's update of [KE, n)
-                M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));
-                lo_pending = false;
-            }
             if ((rc = laswp(K0, JB, KE, n, H))) return rc;                 // the outer panel's interchanges, right
             for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
                 const int jb = std::min(NB, KE - k0);
@@ -1203,7 +1209,6 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             }
         }
     }
-    if (lo_pending) M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));
     M25_CHECK(cudaEventRecord(ev_end, H));                           // the caller's stream waits for both
     M25_CHECK(cudaStreamWaitEvent(s, ev_end, 0));
     return M25_OK;

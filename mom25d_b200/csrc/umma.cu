@@ -246,10 +246,10 @@ __global__ void k_split_A(const float *L, long lda, int M, int K, int Kp, float 
         float r0a = z.x, r0b = -z.y, r1a = z.y, r1b = z.x;
         float h;
         size_t o0 = (size_t)(2 * m) * Kp + 2 * k, o1 = o0 + Kp;
-        h = tf32_rna(r0a); Ahi[o0] = h; Alo[o0] = r0a - h;
-        h = tf32_rna(r0b); Ahi[o0 + 1] = h; Alo[o0 + 1] = r0b - h;
-        h = tf32_rna(r1a); Ahi[o1] = h; Alo[o1] = r1a - h;
-        h = tf32_rna(r1b); Ahi[o1 + 1] = h; Alo[o1 + 1] = r1b - h;
+        h = tf32_rna(r0a); Ahi[o0] = h; Alo[o0] = tf32_rna(r0a - h);
+        h = tf32_rna(r0b); Ahi[o0 + 1] = h; Alo[o0 + 1] = tf32_rna(r0b - h);
+        h = tf32_rna(r1a); Ahi[o1] = h; Alo[o1] = tf32_rna(r1a - h);
+        h = tf32_rna(r1b); Ahi[o1 + 1] = h; Alo[o1 + 1] = tf32_rna(r1b - h);
     }
 }
 
@@ -261,7 +261,7 @@ __global__ void k_split_B(const float *U, long lda, int K, int N, int Kp, float 
     int n = e / Kp, j = e % Kp;
     float x = j < 2 * K ? U[(size_t)n * 2 * lda + j] : 0.f;
     float h = tf32_rna(x);
-    Bhi[e] = h; Blo[e] = x - h;
+    Bhi[e] = h; Blo[e] = tf32_rna(x - h);
 }
 
 typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,

@@ -138,3 +138,44 @@ def test_backend_factor_solve_download(dt):
     be.release()
     with pytest.raises(RuntimeError):
         be.solve(R)
+
+
+@pytest.mark.parametrize('dt', [np.complex64, np.complex128])
+def test_backend_pivoting_over_many_outer_panels(dt):
+    """A Gaussian matrix without a diagonal boost (row interchanges in nearly every column) over a dozen outer
+    panels of 256 columns, so that the interchanges of each panel meet the trailing update of the previous one
+    that runs beside it: the solve's backward error ||Z x - r|| / (||Z|| ||x||) at the factor's round-off."""
+    from mom25d_b200.backend import CudaBackend
+    n = 3000
+    rng = np.random.default_rng(21)
+    Z = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(dt)
+    be = CudaBackend()
+    be.factor(np.ascontiguousarray(Z))
+    _, piv = be.download()
+    assert np.count_nonzero(piv != np.arange(n)) > n // 2
+    R = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
+    X = be.solve(R)
+    Zc = Z.astype(complex)
+    berr = np.linalg.norm(Zc @ X - R) / (np.linalg.norm(Zc) * np.linalg.norm(X))
+    assert berr < (5e-6 if dt == np.complex64 else 1e-14), berr     # LAPACK in complex64: 8.6e-7
+    be.release()
+
+
+@pytest.mark.parametrize('dt', [np.complex64, np.complex128])
+def test_lookahead_factor_equals_the_in_order_one(dt, monkeypatch):
+    """The look-ahead LU (the next outer panel factored while the rest of the previous trailing update runs on a
+    second stream) gives the same bits as the same steps on one stream (M25_LOOKAHEAD=0): no step reads what the
+    other stream writes."""
+    from mom25d_b200.backend import CudaBackend
+    n = 2000
+    rng = np.random.default_rng(22)
+    Z = np.ascontiguousarray((rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(dt))
+    out = []
+    for la in ('1', '0', '1'):
+        monkeypatch.setenv('M25_LOOKAHEAD', la)
+        be = CudaBackend()
+        be.factor(Z)
+        out.append(be.download())
+        be.release()
+    for lu, piv in out[1:]:
+        assert np.array_equal(piv, out[0][1]) and np.array_equal(lu, out[0][0])
