@@ -26,6 +26,7 @@ size_t m25_umma_workspace(int n, int nb);
 #define NB 64
 #define NB2 256
 #define PANEL_THREADS 256
+static_assert(PANEL_THREADS >= 2 * NB, "the panel's row copies take a thread a column for two rows");
 
 struct PanelWork {
     double *cand_val;     // [2][G]
@@ -33,141 +34,301 @@ struct PanelWork {
     double *cand_row;     // [2][G][NB] complex (as R pairs; sized for double)
     double *drow;         // [2][NB] complex
     GridBarrier bar;
-    unsigned *gen;        // [2][G]: the column (+ 1) whose candidate a CTA has published (k_panel_smem)
+    unsigned *gen;        // [2][G]
+    unsigned long long *ll_cand;   // [2][G][LL_REC] flagged words: a block's candidate |re| + |im| and row
+    unsigned long long *ll_row;    // [2][G][4 NB]: its candidate row
+    unsigned long long *ll_drow;   // [2][4 NB]: the diagonal row
 };
 
-// The panel with each block's rows held in shared memory for the whole panel (Ps[c * cs + i], row r0 + i): the
-// per-column work is shared-memory bound and parallel over (row, column); global memory is read once and written
-// once. Used whenever the rows fit (cs * jb * sizeof(complex) <= the opt-in shared memory).
+// The panel's exchange records: 64-bit words of a 32-bit payload and a 32-bit flag (the column + 1 it belongs
+// to), written and read whole (a naturally aligned 64-bit access is single-copy atomic), so that a reader that
+// sees the flag sees the payload: no fence, no separate ready flag, one round trip to L2 per exchange.
+__device__ __forceinline__ void ll_put(unsigned long long *p, unsigned payload, unsigned flag)
+{
+    const unsigned long long w = ((unsigned long long)flag << 32) | payload;
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ unsigned long long ll_get(const unsigned long long *p)
+{
+    unsigned long long w;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+// waits until the K words p[0], p[stride], ... carry flag; their payloads in out. Bounded: false after about 2^22
+// polls or once another block has reported an error.
+template <int K>
+__device__ __forceinline__ bool ll_wait(const unsigned long long *p, int stride, unsigned flag, unsigned *out,
+                                        const int *err)
+{
+    long it = 0;
+    for (;;) {
+        bool all = true;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const unsigned long long w = ll_get(p + (size_t)q * stride);
+            out[q] = (unsigned)w;
+            all = all && (unsigned)(w >> 32) == flag;
+        }
+        if (all) return true;
+        if ((++it & 1023) == 0 && (it > (1L << 22) || *(volatile const int *)err)) return false;
+    }
+}
+
+#ifdef M25_PANEL_TIMING
+// per-phase SM cycles of the panel kernel (thread 0 of every block), summed over blocks and launches, with the
+// count of block-launches in the last slot: a measurement build only
+__device__ unsigned long long g_panel_phase[8];
+#define PANEL_T(q)                                                                                                     \
+    do {                                                                                                               \
+        if (threadIdx.x == 0) {                                                                                        \
+            const long long t_ = clock64();                                                                            \
+            pt_acc[q] += t_ - pt_last;                                                                                 \
+            pt_last = t_;                                                                                              \
+        }                                                                                                              \
+    } while (0)
+#define PANEL_T_BEGIN                                                                                                  \
+    unsigned long long pt_acc[7] = {0, 0, 0, 0, 0, 0, 0};                                                              \
+    long long pt_last = clock64()
+#define PANEL_T_END                                                                                                    \
+    do {                                                                                                               \
+        if (threadIdx.x == 0) {                                                                                        \
+            for (int q_ = 0; q_ < 7; ++q_) atomicAdd(&g_panel_phase[q_], pt_acc[q_]);                                  \
+            atomicAdd(&g_panel_phase[7], 1ull);                                                                        \
+        }                                                                                                              \
+    } while (0)
+extern "C" int m25_panel_timing(unsigned long long *out8)
+{
+    return cudaMemcpyFromSymbol(out8, g_panel_phase, sizeof(unsigned long long) * 8) == cudaSuccess ? 0 : 1;
+}
+#else
+#define PANEL_T(q)
+#define PANEL_T_BEGIN
+#define PANEL_T_END
+#endif
+
+#define PANEL_NONE 0x7fffffff
+#define LL_REC 32             // words a candidate record (256 bytes: polled by every block, one record a line pair)
+
+// The largest |re| + |im| and its row over a warp (the first row on ties: izamax / icamax)
+template <typename R>
+__device__ __forceinline__ void warp_argmax(R &v, int &row)
+{
+    for (int o = 16; o; o >>= 1) {
+        const R ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int orow = __shfl_xor_sync(0xffffffffu, row, o);
+        if (ov > v || (ov == v && orow < row)) { v = ov; row = orow; }
+    }
+}
+
+// The panel (GEPP over jb <= NB columns k0 .., rows k0 .. n) with each block's rows in shared memory for the whole
+// panel (Ps[c * cs + i] is row r0 + i, column k0 + c): global memory is read once and written once. Per column j:
+// (1) the block's candidate; (2) warp 0 brings the candidate row and the diagonal row (where the block holds it) up
+// to date and publishes them with the candidate; (3) the rest of the previous column's rank-1 update (columns
+// j + 1 ..), deferred to here so that it runs while the exchange is in flight; (4) every block's candidate read and
+// reduced; (5) the pivot row and the diagonal row (from the block's own shared memory where it holds them);
+// (6) the interchange, the scaling of column j and the update of column j + 1 only, which yields the next
+// candidates. Two round trips to L2 and three block barriers a column; the arithmetic of every entry is that of
+// the unpipelined order (a -= l U, once per column, in column order).
 template <typename R>
 __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, int n, int k0, int jb, int *ipiv,
                                                               PanelWork pw, int *err)
 {
     typedef cpx<R> C;
+    constexpr int WPC = sizeof(C) / 4;                    // 32-bit words a complex number
+    constexpr int VW = sizeof(R) / 4;                     // 32-bit words of |re| + |im|
+    constexpr int NWARP = PANEL_THREADS / 32;
     extern __shared__ unsigned char panel_raw[];
     C *Ps = reinterpret_cast<C *>(panel_raw);
-    const unsigned G = gridDim.x;
-    const int b = blockIdx.x, tid = threadIdx.x;
+    const unsigned *P32 = reinterpret_cast<const unsigned *>(Ps);
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int rows = n - k0;
     const int cs = (rows + G - 1) / G;
     const int r0 = k0 + b * cs, r1 = min(n, r0 + cs);
     const int nr = max(0, r1 - r0);
-    __shared__ C U[NB], D[NB];
-    __shared__ double sv[PANEL_THREADS / 32];
-    __shared__ int si[PANEL_THREADS / 32];
-    __shared__ int s_p, s_fail;
-    __shared__ int sw[PANEL_THREADS / 32];
-    __shared__ C s_recip;
-    C *cand_row = reinterpret_cast<C *>(pw.cand_row);
-    C *drow = reinterpret_cast<C *>(pw.drow);
+    const int PW = jb * WPC;                              // payload words of one panel row
+    __shared__ __align__(16) C U[NB], D[NB];
+    __shared__ R sv[NWARP], sv2[NWARP];
+    __shared__ int si[NWARP], si2[NWARP], sw2[NWARP];
+    __shared__ int s_fail;
+    PANEL_T_BEGIN;
     for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
         int c = e / nr, i = e % nr;
         Ps[c * cs + i] = ldc<R>(A, (size_t)(k0 + c) * lda + r0 + i);
     }
     if (tid == 0) s_fail = 0;
     __syncthreads();
+    PANEL_T(0);
+    R best = -1;                                          // this thread's candidate for column 0
+    int bi = PANEL_NONE;
+    for (int i = tid; i < nr; i += PANEL_THREADS) {
+        const R v = abs1(Ps[i]);
+        if (v > best) { best = v; bi = r0 + i; }
+    }
     for (int j = 0; j < jb; ++j) {
         const int col = k0 + j, par = j & 1;
-        double best = -1.0;
-        int bi = 0x7fffffff;
-        for (int i = max(0, col - r0) + tid; i < nr; i += PANEL_THREADS) {
-            double v = abs1(Ps[j * cs + i]);
-            if (v > best) { best = v; bi = r0 + i; }
-        }
-        for (int o = 16; o; o >>= 1) {
-            double ov = __shfl_xor_sync(0xffffffffu, best, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        if ((tid & 31) == 0) { sv[tid >> 5] = best; si[tid >> 5] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            for (int w = 1; w < PANEL_THREADS / 32; ++w)
-                if (sv[w] > best || (sv[w] == best && si[w] < bi)) { best = sv[w]; bi = si[w]; }
-            pw.cand_val[par * G + b] = best;
-            pw.cand_idx[par * G + b] = bi;
-            s_p = bi;
-        }
-        __syncthreads();
-        if (s_p != 0x7fffffff && tid < jb) cand_row[((size_t)par * G + b) * NB + tid] = Ps[tid * cs + (s_p - r0)];
-        if (col >= r0 && col < r1 && tid < jb) drow[par * NB + tid] = Ps[tid * cs + (col - r0)];
-        // the exchange of this column's candidates: no counter, no second round trip. Each CTA publishes its
-        // record (candidate, its row, the diagonal row) with a per-CTA generation; thread w < G waits for CTA w's
-        // generation and reads its candidate, and the CTA reduces them itself
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            atomicExch(pw.gen + par * G + b, (unsigned)(j + 1));
-        }
-        double bv = -1.0;
-        int bw = -1, brow = 0x7fffffff;
-        if (tid < (int)G) {
-            long it = 0;
-            bool ok = true;
-            while (ld_acquire_u32(pw.gen + par * G + tid) != (unsigned)(j + 1)) {
-                if ((++it & 1023) == 0 && (it > (1L << 22) || *(volatile int *)err)) { ok = false; break; }
+        const unsigned flag = (unsigned)col + 1u;
+        const bool own_col = col >= r0 && col < r1;
+        // (1) the block's candidate
+        warp_argmax(best, bi);
+        if (lane == 0) { sv[wid] = best; si[wid] = bi; }
+        __syncthreads();                                  // (column j is complete for every row >= col)
+        PANEL_T(1);
+        best = sv[0]; bi = si[0];
+        for (int w = 1; w < NWARP; ++w)
+            if (sv[w] > best || (sv[w] == best && si[w] < bi)) { best = sv[w]; bi = si[w]; }
+        const int ec = own_col ? col - r0 : -1;                          // rows brought up to date eagerly
+        const int eb = (bi != PANEL_NONE && bi != col) ? bi - r0 : -1;
+        // (2) warp 0: the previous column's update of columns j + 1 .. of those rows, then the block's record
+        if (wid == 0) {
+            if (j > 0) {
+                for (int q = 0; q < 2; ++q) {
+                    const int e = q ? eb : ec;
+                    if (e < 0) continue;
+                    const C lp = Ps[(j - 1) * cs + e];
+                    for (int c = j + 1 + lane; c < jb; c += 32) {
+                        C a = Ps[c * cs + e];
+                        cfms<R>(a, lp, U[c]);
+                        Ps[c * cs + e] = a;
+                    }
+                }
+                __syncwarp();
             }
-            if (!ok) { s_fail = 1; dev_error(err, M25_DEV_TIMEOUT); }
-            else {
-                const double v = __ldcg(pw.cand_val + par * G + tid);
-                const int ri = __ldcg(pw.cand_idx + par * G + tid);
-                if (ri != 0x7fffffff) { bv = v; bw = tid; brow = ri; }
+            unsigned long long *rec = pw.ll_cand + ((size_t)par * G + b) * LL_REC;
+            if (lane == 0) {
+                const unsigned *bv32 = reinterpret_cast<const unsigned *>(&best);
+#pragma unroll
+                for (int q = 0; q < VW; ++q) ll_put(rec + q, bv32[q], flag);
+                ll_put(rec + VW, (unsigned)bi, flag);
+            }
+            for (int t = lane; t < PW; t += 32) {
+                const int c = t / WPC, q = t % WPC;
+                if (bi != PANEL_NONE)
+                    ll_put(pw.ll_row + ((size_t)par * G + b) * (4 * NB) + t,
+                           P32[((size_t)c * cs + (bi - r0)) * WPC + q], flag);
+                if (own_col)
+                    ll_put(pw.ll_drow + (size_t)par * (4 * NB) + t, P32[((size_t)c * cs + (col - r0)) * WPC + q], flag);
             }
         }
-        for (int o = 16; o; o >>= 1) {
-            double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            int ow = __shfl_xor_sync(0xffffffffu, bw, o), orow = __shfl_xor_sync(0xffffffffu, brow, o);
-            if (ov > bv || (ov == bv && orow < brow)) { bv = ov; bw = ow; brow = orow; }
+        // (3) the previous column's update of columns j + 1 .. for the other rows >= col: two threads a row
+        // (adjacent lanes), columns j + 1 + sub, j + 3 + sub, ..., four at a time with their loads issued together
+        if (j > 0) {
+            const int sub = tid & 1;
+            for (int i = max(0, col - r0) + (tid >> 1); i < nr; i += PANEL_THREADS / 2) {
+                if (i == ec || i == eb) continue;
+                const C lp = Ps[(j - 1) * cs + i];
+                int c = j + 1 + sub;
+                for (; c + 6 < jb; c += 8) {
+                    C a0 = Ps[c * cs + i], a1 = Ps[(c + 2) * cs + i], a2 = Ps[(c + 4) * cs + i],
+                      a3 = Ps[(c + 6) * cs + i];
+                    const C u0 = U[c], u1 = U[c + 2], u2 = U[c + 4], u3 = U[c + 6];
+                    cfms<R>(a0, lp, u0); cfms<R>(a1, lp, u1); cfms<R>(a2, lp, u2); cfms<R>(a3, lp, u3);
+                    Ps[c * cs + i] = a0; Ps[(c + 2) * cs + i] = a1;
+                    Ps[(c + 4) * cs + i] = a2; Ps[(c + 6) * cs + i] = a3;
+                }
+                for (; c < jb; c += 2) {
+                    C a = Ps[c * cs + i];
+                    cfms<R>(a, lp, U[c]);
+                    Ps[c * cs + i] = a;
+                }
+            }
         }
-        if ((tid & 31) == 0) { sv[tid >> 5] = bv; si[tid >> 5] = brow; sw[tid >> 5] = bw; }
-        __syncthreads();
+        // (4) every block's candidate
+        R bv = -1;
+        int brow = PANEL_NONE, bw = -1;
+        if (tid < G) {
+            unsigned wv[VW + 1];
+            if (!ll_wait<VW + 1>(pw.ll_cand + ((size_t)par * G + tid) * LL_REC, 1, flag, wv, err)) {
+                s_fail = 1;
+                dev_error(err, M25_DEV_TIMEOUT);
+            } else if ((int)wv[VW] != PANEL_NONE) {
+                R v;
+                memcpy(&v, wv, sizeof(R));
+                bv = v; brow = (int)wv[VW]; bw = tid;
+            }
+        }
+        for (int o = 16; o; o >>= 1) {
+            const R ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, brow, o), ow = __shfl_xor_sync(0xffffffffu, bw, o);
+            if (ov > bv || (ov == bv && orow < brow)) { bv = ov; brow = orow; bw = ow; }
+        }
+        if (lane == 0) { sv2[wid] = bv; si2[wid] = brow; sw2[wid] = bw; }
+        __syncthreads();                                  // (and the deferred update is complete)
+        PANEL_T(2);
         if (s_fail) return;
-        if (tid == 0) {
-            for (int w = 1; w < PANEL_THREADS / 32; ++w)
-                if (sv[w] > bv || (sv[w] == bv && si[w] < brow)) { bv = sv[w]; bw = sw[w]; brow = si[w]; }
-            si[0] = bw;
-            s_p = brow;
-            if (b == 0 && bw >= 0) ipiv[col] = brow;
-        }
-        __syncthreads();
-        const int wb = si[0], p = s_p;
-        if (wb < 0) { dev_error(err, M25_DEV_INDEX); return; }
-        if (tid < jb) {                                             // other CTAs' rows: past L1, one load each
-            typedef typename vec2_of<R>::type V2;
-            const V2 u = __ldcg(reinterpret_cast<const V2 *>(cand_row + ((size_t)par * G + wb) * NB + tid));
-            const V2 d = __ldcg(reinterpret_cast<const V2 *>(drow + par * NB + tid));
-            U[tid] = mk<R>(u.x, u.y);
-            D[tid] = mk<R>(d.x, d.y);
-        }
-        __syncthreads();
-        if (tid < jb) {
-            if (col >= r0 && col < r1) Ps[tid * cs + (col - r0)] = U[tid];
-            if (p != col && p >= r0 && p < r1) Ps[tid * cs + (p - r0)] = D[tid];
-        }
-        if (tid == 0) {
-            C piv = U[j];
-            if (piv.x == 0 && piv.y == 0) { dev_error(err, M25_DEV_ZEROPIV); s_recip = mk<R>(0, 0); }
-            else s_recip = cdiv<R>(mk<R>(1, 0), piv);
-        }
-        __syncthreads();
-        const C rc = s_recip;
-        const int i0 = max(0, col + 1 - r0), na = nr - i0;
-        for (int i = i0 + tid; i < nr; i += PANEL_THREADS) Ps[j * cs + i] = Ps[j * cs + i] * rc;
-        __syncthreads();
-        const int nc = jb - j - 1;
-        if (na > 0)
-            for (int e = tid; e < na * nc; e += PANEL_THREADS) {
-                int i = i0 + e % na, c = j + 1 + e / na;
-                C a = Ps[c * cs + i];
-                cfms<R>(a, Ps[j * cs + i], U[c]);
-                Ps[c * cs + i] = a;
+        bv = sv2[0]; brow = si2[0]; bw = sw2[0];
+        for (int w = 1; w < NWARP; ++w)
+            if (sv2[w] > bv || (sv2[w] == bv && si2[w] < brow)) { bv = sv2[w]; brow = si2[w]; bw = sw2[w]; }
+        if (bw < 0 || bw >= G) { if (tid == 0) dev_error(err, M25_DEV_INDEX); return; }
+        const int p = brow;
+        if (b == 0 && tid == 0) ipiv[col] = p;
+        // (5) every block: U[j ..]; the block that holds row col: all of U; the block that holds row p: D. A row
+        // the block holds comes from its own shared memory: at most one read from L2 a word
+        if (tid < PW) {
+            const int c = tid / WPC, q = tid % WPC;
+            const bool own_p = b == bw, need_u = own_col || tid >= j * WPC;
+            unsigned u = 0, d = 0;
+            bool ok = true;
+            if (own_p) {
+                u = P32[((size_t)c * cs + (p - r0)) * WPC + q];
+                if (own_col) d = P32[((size_t)c * cs + (col - r0)) * WPC + q];
+                else ok = ll_wait<1>(pw.ll_drow + (size_t)par * (4 * NB) + tid, 0, flag, &d, err);
+            } else if (need_u) {
+                ok = ll_wait<1>(pw.ll_row + ((size_t)par * G + bw) * (4 * NB) + tid, 0, flag, &u, err);
             }
+            if (!ok) {
+                s_fail = 1;
+                dev_error(err, M25_DEV_TIMEOUT);
+            } else {
+                if (own_p || need_u) reinterpret_cast<unsigned *>(U)[tid] = u;
+                if (own_p) reinterpret_cast<unsigned *>(D)[tid] = d;
+            }
+        }
         __syncthreads();
+        PANEL_T(3);
+        if (s_fail) return;
+        // (6) rows col and p interchanged (whole panel rows), column j scaled by 1 / pivot, column j + 1 updated
+        // (the rest of this column's update is deferred to the next column's step 3); the next candidates
+        const C piv = U[j];
+        C rc;
+        if (piv.x == 0 && piv.y == 0) {
+            if (b == 0 && tid == 0) dev_error(err, M25_DEV_ZEROPIV);
+            rc = mk<R>(0, 0);
+        } else {
+            rc = cdiv<R>(mk<R>(1, 0), piv);
+        }
+        // the interchanged rows' copies spread over the block (one thread copying a row alone would hold every
+        // other block up at the next exchange); the thread of row p writes its columns j and j + 1 itself
+        {
+            const int e = tid % NB, half = tid / NB;
+            if (e < jb) {
+                if (half == 0 && own_col) Ps[e * cs + (col - r0)] = U[e];
+                if (half == 1 && b == bw && p != col && e != j && e != j + 1) Ps[e * cs + (p - r0)] = D[e];
+            }
+        }
+        best = -1; bi = PANEL_NONE;
+        for (int i = max(0, col - r0) + tid; i < nr; i += PANEL_THREADS) {
+            const int row = r0 + i;
+            if (row == col) continue;
+            const bool isp = row == p;
+            const C l = (isp ? D[j] : Ps[j * cs + i]) * rc;
+            Ps[j * cs + i] = l;
+            if (j + 1 < jb) {
+                C a = isp ? D[j + 1] : Ps[(j + 1) * cs + i];
+                cfms<R>(a, l, U[j + 1]);
+                Ps[(j + 1) * cs + i] = a;
+                const R v = abs1(a);
+                if (v > best) { best = v; bi = row; }
+            }
+        }
+        PANEL_T(4);
     }
+    __syncthreads();
     for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
         int c = e / nr, i = e % nr;
         stc<R>(A, (size_t)(k0 + c) * lda + r0 + i, Ps[c * cs + i]);
     }
+    PANEL_T(5);
+    PANEL_T_END;
 }
 
 // The same with the rows in global memory (when a block's rows do not fit in shared memory).
@@ -325,6 +486,70 @@ __global__ void __launch_bounds__(256) k_trsm(R *A, long lda, int k0, int jb, lo
     if (live)
         for (int k = g; k < jb; k += 4) stc<R>(A, (size_t)c * lda + k0 + k, X[k * 64 + cl]);
 }
+
+// The same for complex64 and a full panel (jb = NB = 64) without a barrier inside the substitution: a warp solves 32
+// columns, one a lane, the lane's column in registers (64 complex), L11 in shared memory read as broadcasts. The
+// columns are staged through shared memory (a column's stride NB + 1: the lanes' reads of their own columns fall in
+// different banks) so that every global load and store is a warp's 256 contiguous bytes. The arithmetic and its
+// order are those of k_trsm (row i's multiple subtracted from the rows below, i ascending).
+#define T64_WARPS 4
+__global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64_c64(float *A, long lda, int k0, long c0, long c1)
+{
+    typedef cpx<float> C;
+    constexpr int XS = NB + 1;
+    extern __shared__ __align__(16) unsigned char t64_raw[];
+    C *L = reinterpret_cast<C *>(t64_raw);                   // L[i * NB + k] = L11(k, i)
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    C *Xs = L + NB * NB + (size_t)w * 32 * XS;
+    const float2 *A2 = reinterpret_cast<const float2 *>(A);
+    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+        const int i = e / NB, k = e % NB;
+        const float2 v = A2[(size_t)(k0 + i) * lda + k0 + k];
+        L[e] = mk<float>(v.x, v.y);
+    }
+    const long cbase = c0 + ((long)blockIdx.x * T64_WARPS + w) * 32;
+    for (int c8 = 0; c8 < 32; c8 += 8) {                    // 16 loads in flight a lane
+        float2 v[8][2];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const long c = cbase + c8 + q;
+            if (c < c1) {
+                const float2 *src = A2 + (size_t)c * lda + k0;
+                v[q][0] = src[lane];
+                v[q][1] = src[lane + 32];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (cbase + c8 + q < c1) {
+                Xs[(c8 + q) * XS + lane] = mk<float>(v[q][0].x, v[q][0].y);
+                Xs[(c8 + q) * XS + lane + 32] = mk<float>(v[q][1].x, v[q][1].y);
+            }
+    }
+    __syncthreads();
+    C x[NB];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) x[k] = Xs[lane * XS + k];
+#pragma unroll
+    for (int i = 0; i < NB - 1; ++i) {
+#pragma unroll
+        for (int k = i + 1; k < NB; ++k) cfms<float>(x[k], L[i * NB + k], x[i]);
+    }
+#pragma unroll
+    for (int k = 0; k < NB; ++k) Xs[lane * XS + k] = x[k];
+    __syncwarp();
+    float2 *D2 = reinterpret_cast<float2 *>(A);
+    for (int cc = 0; cc < 32; ++cc) {
+        const long c = cbase + cc;
+        if (c < c1) {
+            float2 *dst = D2 + (size_t)c * lda + k0;
+            const C v0 = Xs[cc * XS + lane], v1 = Xs[cc * XS + lane + 32];
+            dst[lane] = make_float2(v0.x, v0.y);
+            dst[lane + 32] = make_float2(v1.x, v1.y);
+        }
+    }
+}
+static constexpr size_t T64_SMEM = sizeof(cpx<float>) * (NB * NB + (size_t)T64_WARPS * 32 * (NB + 1));
 
 // C (M x N) -= A (M x K) B (K x N), all column-major complex inside the factor (lda). A 128 x 64 tile per block of
 // 256 threads, each 8 x 4 outputs; K staged BK at a time through two shared-memory buffers, the next slice loaded
@@ -1044,6 +1269,7 @@ extern "C" size_t m25_getrf_workspace(int n, int single)
     b += 2 * (size_t)G * NB * 2 * sizeof(double) + 256;             // cand_row
     b += 2 * NB * 2 * sizeof(double) + 256;                         // drow
     b += (2 + 2 * (size_t)G) * sizeof(unsigned) + 256;             // barrier, the panel's generations
+    b += (2 * (size_t)G * (LL_REC + 4 * NB) + 2 * 4 * NB) * 8 + 256; // the flagged exchange records
     if (single) b += 2 * (m25_umma_workspace(n, NB) + 256);          // one a stream (look-ahead)
     (void)n;
     return b;
@@ -1093,6 +1319,10 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     pw.cand_row = (double *)take(2 * (size_t)G * NB * 2 * sizeof(double));
     pw.drow = (double *)take(2 * NB * 2 * sizeof(double));
     unsigned *bar = (unsigned *)take((2 + 2 * (size_t)G) * sizeof(unsigned));
+    const size_t ll_bytes = (2 * (size_t)G * (LL_REC + 4 * NB) + 2 * 4 * NB) * 8;
+    pw.ll_cand = (unsigned long long *)take(ll_bytes);
+    pw.ll_row = pw.ll_cand + 2 * (size_t)G * LL_REC;
+    pw.ll_drow = pw.ll_row + 2 * (size_t)G * 4 * NB;
     void *umma_work0 = take(0);
     size_t umma_bytes = (work_bytes - ((unsigned char *)umma_work0 - (unsigned char *)work)) / 2 / 256 * 256;
     void *umma_work1 = (unsigned char *)umma_work0 + umma_bytes;
@@ -1109,15 +1339,22 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     M25_CHECK(cudaStreamWaitEvent(H, ev_start, 0));
     M25_CHECK(cudaStreamWaitEvent(Lo, ev_start, 0));
     M25_CHECK(cudaMemsetAsync(ipiv, 0xff, sizeof(int) * (size_t)n, H));      // -1 until the panel sets it
+    M25_CHECK(cudaMemsetAsync(pw.ll_cand, 0, ll_bytes, H));         // flags 0: no column's (they are column + 1)
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
     M25_CHECK(cudaFuncSetAttribute(k_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+    M25_CHECK(cudaFuncSetAttribute(k_trsm64_c64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T64_SMEM));
     int smem_optin = 0, dev = 0;
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const int smem_cap = smem_optin - 4096;                          // (the kernel's static shared memory)
     M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
-    int gmax = G;                                                    // blocks of the panel (M25_PANEL_BLOCKS: tuning)
+    // Blocks of the panel: few enough that the cooperative launch finds its SMs quickly while the other stream's
+    // update holds the rest (the exchange costs about the same from 37 to 148 blocks), but at least as many as
+    // the panel's rows need to fit in shared memory (M25_PANEL_BLOCKS: tuning)
+    int gmax = std::min(G, 32);
     if (const char *e = getenv("M25_PANEL_BLOCKS")) gmax = std::max(1, std::min(G, atoi(e)));
+    const int rows_cap = (int)((size_t)smem_cap / (sizeof(cpx<R>) * NB));   // a block's rows in shared memory
+    const int gcap = std::min(G, PANEL_THREADS);                     // a thread of each block reads a block's record
     int nb2 = NB2;                                                   // outer panel (M25_NB2: tuning, a multiple of NB)
     if (const char *e = getenv("M25_NB2")) nb2 = std::max(NB, atoi(e) / NB * NB);
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
@@ -1130,6 +1367,13 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     };
     auto trsm = [&](int k0, int jb, long c0, long c1, cudaStream_t cs) -> int {
         if (c1 <= c0) return M25_OK;
+        if (sizeof(R) == 4 && jb == NB) {
+            const long per = 32L * T64_WARPS;
+            k_trsm64_c64<<<(unsigned)((c1 - c0 + per - 1) / per), 32 * T64_WARPS, T64_SMEM, cs>>>((float *)A, lda, k0,
+                                                                                                 c0, c1);
+            M25_LAUNCH_CHECK("k_trsm64_c64");
+            return M25_OK;
+        }
         k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, cs>>>(A, lda, k0, jb, c0, c1);
         M25_LAUNCH_CHECK("k_trsm");
         return M25_OK;
@@ -1167,6 +1411,7 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
         for (int k0 = K0; k0 < KE; k0 += NB) {
             const int jb = std::min(NB, KE - k0);
             int Gp = std::min(gmax, std::max(1, (n - k0 + 31) / 32));
+            Gp = std::min(gcap, std::max(Gp, (n - k0 + rows_cap - 1) / rows_cap));
             const int cs = (n - k0 + Gp - 1) / Gp;
             const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
             M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), H));
