@@ -487,34 +487,41 @@ __global__ void __launch_bounds__(256) k_trsm(R *A, long lda, int k0, int jb, lo
         for (int k = g; k < jb; k += 4) stc<R>(A, (size_t)c * lda + k0 + k, X[k * 64 + cl]);
 }
 
-// The same for complex64 and a full panel (jb = NB = 64) without a barrier inside the substitution: a warp solves 32
+// The same for a full panel (jb = NB = 64) without a barrier inside the substitution: a warp solves 32
 // columns, one a lane, the lane's column in registers (64 complex), L11 in shared memory read as broadcasts. The
 // columns are staged through shared memory (a column's stride NB + 1: the lanes' reads of their own columns fall in
 // different banks) so that every global load and store is a warp's 256 contiguous bytes. The arithmetic and its
 // order are those of k_trsm (row i's multiple subtracted from the rows below, i ascending).
-#define T64_WARPS 4
-__global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64_c64(float *A, long lda, int k0, long c0, long c1)
+template <typename R, int T64_WARPS>
+__global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64(R *A, long lda, int k0, long c0, long c1)
 {
-    typedef cpx<float> C;
+    typedef cpx<R> C;
+    typedef typename vec2_of<R>::type V;
     constexpr int XS = NB + 1;
     extern __shared__ __align__(16) unsigned char t64_raw[];
     C *L = reinterpret_cast<C *>(t64_raw);                   // L[i * NB + k] = L11(k, i)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     C *Xs = L + NB * NB + (size_t)w * 32 * XS;
-    const float2 *A2 = reinterpret_cast<const float2 *>(A);
-    for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-        const int i = e / NB, k = e % NB;
-        const float2 v = A2[(size_t)(k0 + i) * lda + k0 + k];
-        L[e] = mk<float>(v.x, v.y);
+    const V *A2 = reinterpret_cast<const V *>(A);
+    static_assert(NB * NB % (8 * 32 * T64_WARPS) == 0, "L11 in whole batches");
+    for (int e0 = threadIdx.x; e0 < NB * NB; e0 += 8 * 32 * T64_WARPS) {     // 8 loads in flight a thread
+        V v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = e0 + q * 32 * T64_WARPS, i = e / NB, k = e % NB;
+            v[q] = A2[(size_t)(k0 + i) * lda + k0 + k];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) L[e0 + q * 32 * T64_WARPS] = mk<R>(v[q].x, v[q].y);
     }
     const long cbase = c0 + ((long)blockIdx.x * T64_WARPS + w) * 32;
     for (int c8 = 0; c8 < 32; c8 += 8) {                    // 16 loads in flight a lane
-        float2 v[8][2];
+        V v[8][2];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const long c = cbase + c8 + q;
             if (c < c1) {
-                const float2 *src = A2 + (size_t)c * lda + k0;
+                const V *src = A2 + (size_t)c * lda + k0;
                 v[q][0] = src[lane];
                 v[q][1] = src[lane + 32];
             }
@@ -522,34 +529,58 @@ __global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64_c64(float *A, long ld
 #pragma unroll
         for (int q = 0; q < 8; ++q)
             if (cbase + c8 + q < c1) {
-                Xs[(c8 + q) * XS + lane] = mk<float>(v[q][0].x, v[q][0].y);
-                Xs[(c8 + q) * XS + lane + 32] = mk<float>(v[q][1].x, v[q][1].y);
+                Xs[(c8 + q) * XS + lane] = mk<R>(v[q][0].x, v[q][0].y);
+                Xs[(c8 + q) * XS + lane + 32] = mk<R>(v[q][1].x, v[q][1].y);
             }
     }
     __syncthreads();
-    C x[NB];
+    // by blocks of 16 rows (the unrolled code of two 16 x 16 steps stays in the instruction cache): the diagonal
+    // block solved in registers, then its multiples subtracted from each block below; every entry still takes its
+    // terms in ascending i
+    C *xs = Xs + lane * XS;
+    for (int d = 0; d < NB / 16; ++d) {
+        C xd[16];
 #pragma unroll
-    for (int k = 0; k < NB; ++k) x[k] = Xs[lane * XS + k];
+        for (int k = 0; k < 16; ++k) xd[k] = xs[d * 16 + k];
 #pragma unroll
-    for (int i = 0; i < NB - 1; ++i) {
+        for (int i = 0; i < 15; ++i) {
 #pragma unroll
-        for (int k = i + 1; k < NB; ++k) cfms<float>(x[k], L[i * NB + k], x[i]);
+            for (int k = i + 1; k < 16; ++k) cfms<R>(xd[k], L[(d * 16 + i) * NB + d * 16 + k], xd[i]);
+        }
+#pragma unroll
+        for (int k = 0; k < 16; ++k) xs[d * 16 + k] = xd[k];
+        for (int e = d + 1; e < NB / 16; ++e) {
+            C xe[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) xe[k] = xs[e * 16 + k];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) cfms<R>(xe[k], L[(d * 16 + i) * NB + e * 16 + k], xd[i]);
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) xs[e * 16 + k] = xe[k];
+        }
     }
-#pragma unroll
-    for (int k = 0; k < NB; ++k) Xs[lane * XS + k] = x[k];
     __syncwarp();
-    float2 *D2 = reinterpret_cast<float2 *>(A);
+    V *D2 = reinterpret_cast<V *>(A);
     for (int cc = 0; cc < 32; ++cc) {
         const long c = cbase + cc;
         if (c < c1) {
-            float2 *dst = D2 + (size_t)c * lda + k0;
+            V *dst = D2 + (size_t)c * lda + k0;
             const C v0 = Xs[cc * XS + lane], v1 = Xs[cc * XS + lane + 32];
-            dst[lane] = make_float2(v0.x, v0.y);
-            dst[lane + 32] = make_float2(v1.x, v1.y);
+            V w0, w1;
+            w0.x = v0.x; w0.y = v0.y; w1.x = v1.x; w1.y = v1.y;
+            dst[lane] = w0;
+            dst[lane + 32] = w1;
         }
     }
 }
-static constexpr size_t T64_SMEM = sizeof(cpx<float>) * (NB * NB + (size_t)T64_WARPS * 32 * (NB + 1));
+template <typename R> constexpr int t64_warps() { return sizeof(R) == 4 ? 4 : 2; }
+template <typename R> constexpr size_t t64_smem()
+{
+    return sizeof(cpx<R>) * (NB * NB + (size_t)t64_warps<R>() * 32 * (NB + 1));
+}
 
 // C (M x N) -= A (M x K) B (K x N), all column-major complex inside the factor (lda). A 128 x 64 tile per block of
 // 256 threads, each 8 x 4 outputs; K staged BK at a time through two shared-memory buffers, the next slice loaded
@@ -1342,7 +1373,8 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     M25_CHECK(cudaMemsetAsync(pw.ll_cand, 0, ll_bytes, H));         // flags 0: no column's (they are column + 1)
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
     M25_CHECK(cudaFuncSetAttribute(k_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
-    M25_CHECK(cudaFuncSetAttribute(k_trsm64_c64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T64_SMEM));
+    M25_CHECK(cudaFuncSetAttribute(k_trsm64<R, t64_warps<R>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)t64_smem<R>()));
     int smem_optin = 0, dev = 0;
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1367,11 +1399,11 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     };
     auto trsm = [&](int k0, int jb, long c0, long c1, cudaStream_t cs) -> int {
         if (c1 <= c0) return M25_OK;
-        if (sizeof(R) == 4 && jb == NB) {
-            const long per = 32L * T64_WARPS;
-            k_trsm64_c64<<<(unsigned)((c1 - c0 + per - 1) / per), 32 * T64_WARPS, T64_SMEM, cs>>>((float *)A, lda, k0,
-                                                                                                 c0, c1);
-            M25_LAUNCH_CHECK("k_trsm64_c64");
+        if (jb == NB) {
+            const long per = 32L * t64_warps<R>();
+            k_trsm64<R, t64_warps<R>()><<<(unsigned)((c1 - c0 + per - 1) / per), (unsigned)per, t64_smem<R>(), cs>>>(
+                A, lda, k0, c0, c1);
+            M25_LAUNCH_CHECK("k_trsm64");
             return M25_OK;
         }
         k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, cs>>>(A, lda, k0, jb, c0, c1);
