@@ -21,10 +21,16 @@ int *m25_dev_err_word();
 
 namespace {
 
-// tile of C' (rows x cols), K floats per stage (16 floats = 64 B rows: 64B swizzle), stages in the ring: three
-// stages in flight while one is multiplied
+// tile of C' (rows x cols), K floats per stage (16 floats = 64 B rows: 64B swizzle). Two stages a CTA, so that two
+// CTAs fit an SM (2 x 97 KB of shared memory, 2 x 256 tensor-memory columns): one's epilogue (C read, updated and
+// written back) runs while the other multiplies, which one CTA with four stages could not do (3.92 -> 3.38 ms for
+// an 18,000 x 18,000 x 256 complex update)
 constexpr int BM = 128, BN = 256, BKF = 16;
-constexpr int STAGES = 4;
+#ifndef M25_UMMA_STAGES
+#define M25_UMMA_STAGES 2
+#endif
+constexpr int STAGES = M25_UMMA_STAGES;
+constexpr int CTAS_PER_SM = STAGES <= 2 ? 2 : 1;           // two CTAs an SM when their stages fit twice
 constexpr int SWZ_BYTES = BKF * 4;                   // the swizzle span: one K row of a stage
 static_assert(SWZ_BYTES == 64 || SWZ_BYTES == 128, "64B or 128B swizzle");
 constexpr int A_BYTES = BM * BKF * 4, B_BYTES = BN * BKF * 4;
@@ -101,7 +107,7 @@ __device__ __forceinline__ float tf32_rna(float x)
     return __uint_as_float(r);
 }
 
-__global__ void __launch_bounds__(128, 1) k_umma_update(float *C, long ldc_f, int Mp, int Nc, int kchunks,
+__global__ void __launch_bounds__(128, CTAS_PER_SM) k_umma_update(float *C, long ldc_f, int Mp, int Nc, int kchunks,
                                                         const __grid_constant__ CUtensorMap mAhi,
                                                         const __grid_constant__ CUtensorMap mAlo,
                                                         const __grid_constant__ CUtensorMap mBhi,
