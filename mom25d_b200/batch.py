@@ -1,0 +1,123 @@
+"""
+mom25d_b200.batch - one board's whole frequency sweep at once: every frequency an independent mixed-precision
+solve, several in flight on one GPU, against the same frequencies solved one after another in FP64.
+
+    python -m mom25d_b200.batch [--freqs 64] [--fmin 1e9] [--fmax 6e9] [--slots 6] [--fp64 64]
+
+The workload is the stub filter board (board.stub_filter_board: three layers 0.2 / 1.0 / 0.2 mm, a 50 ohm line
+40 mm long with an open quarter-wave stub at 2.4 GHz, dmax 0.2 mm, a via port at each line end) at
+linspace(fmin, fmax, freqs).
+
+  - batched: all frequencies are present at the start and go through the serving loop (serve.Server): each slot
+    has its own CUDA stream, host thread and solver, so one frequency's panel factorisation, triangular solves and
+    host synchronisations overlap the others' tensor-core updates. Kept-LU reuse is off (each frequency's result
+    does not depend on the others');
+  - sequential mixed: the reference's sweep (fast.py:996-1118) on one stream, kept complex64 LUs reused within the
+    learnt reach;
+  - FP64: the drop-in path, one frequency after another (each its own complex128 fill and LU).
+
+Reported (one JSON line): solves/s of each (wall clock around the sweep, after a warm-up), the batched-over-FP64
+ratio, and the largest |dS| of both mixed sweeps against FP64 over the frequencies FP64 solved.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from .serve import Request, Server
+
+
+def sweep_requests(key, freqs):
+    """A sweep as requests that have all arrived at the start, in frequency order."""
+    return [Request(i, key, f, 0.0) for i, f in enumerate(freqs)]
+
+
+def batched_sweep(server, key, freqs):
+    """All frequencies through the server at once: (S list in frequency order, wall seconds, requests)."""
+    reqs = sweep_requests(key, freqs)
+    t = time.perf_counter()
+    server.run(reqs)
+    wall = time.perf_counter() - t
+    bad = [r for r in reqs if r.error is not None]
+    if bad:
+        raise RuntimeError(f"batched sweep: {len(bad)} frequencies failed, the first: {bad[0].error}")
+    return [r.S for r in reqs], wall, reqs
+
+
+def sequential_sweep(sim, freqs):
+    """One frequency after another through Simulation.sparams: (S list, wall seconds)."""
+    import torch
+    out = []
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for f in freqs:
+        out.append(sim.sparams(f))
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t
+
+
+def max_dS(A, B):
+    return float(max(np.abs(np.asarray(a) - np.asarray(b)).max() for a, b in zip(A, B)))
+
+
+def run(board, freqs, slots=6, fp64_count=None, sequential_mixed=True):
+    import torch
+    from .sim import Simulation
+    freqs = [float(f) for f in freqs]
+    fp64_count = len(freqs) if fp64_count is None else min(int(fp64_count), len(freqs))
+    key = getattr(board, 'name', 'board')
+    srv = Server({key: board}, slots=slots)
+    N = srv.size(key)
+    # warm-up: a solve on every slot (kernels loaded, solvers, streams and buffers built)
+    batched_sweep(srv, key, [freqs[len(freqs) // 2]] * slots)
+    S_b, wall_b, reqs = batched_sweep(srv, key, freqs)
+    out = dict(workload=f"{key}: N={N} unknowns, {len(freqs)} frequencies linspace({freqs[0] / 1e9:.4g}, "
+                        f"{freqs[-1] / 1e9:.4g} GHz)", unknowns=N, frequencies=len(freqs), slots=slots,
+               batched=dict(solves_per_s=round(len(freqs) / wall_b, 3), wall_s=round(wall_b, 3),
+                            paths={p: sum(r.path == p for r in reqs) for p in sorted({r.path for r in reqs})}))
+    del srv
+    torch.cuda.empty_cache()
+    fsel = freqs[:fp64_count] if fp64_count == len(freqs) else \
+        [freqs[i] for i in np.linspace(0, len(freqs) - 1, fp64_count).round().astype(int)]
+    isel = [freqs.index(f) for f in fsel]
+    sim64 = Simulation.from_board(board, precision='double')
+    sim64.sparams(fsel[0])                                # warm-up
+    S_d, wall_d = sequential_sweep(sim64, fsel)
+    out['fp64'] = dict(solves_per_s=round(len(fsel) / wall_d, 3), wall_s=round(wall_d, 3), frequencies=len(fsel))
+    out['batched_over_fp64'] = round(out['batched']['solves_per_s'] / out['fp64']['solves_per_s'], 3)
+    out['max_dS_batched_vs_fp64'] = max_dS([S_b[i] for i in isel], S_d)
+    del sim64
+    torch.cuda.empty_cache()
+    if sequential_mixed:
+        simm = Simulation.from_board(board, precision='mixed')
+        simm.sparams(freqs[len(freqs) // 2])              # warm-up, then a cold sweep
+        ds = simm.fast
+        ds.kept, ds.reach, ds.t_iter, ds.mixed_failed = [], float(np.log(2.0)), None, 0.0
+        S_m, wall_m = sequential_sweep(simm, freqs)
+        out['sequential_mixed'] = dict(solves_per_s=round(len(freqs) / wall_m, 3), wall_s=round(wall_m, 3))
+        out['max_dS_sequential_mixed_vs_fp64'] = max_dS([S_m[i] for i in isel], S_d)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--freqs', type=int, default=64)
+    ap.add_argument('--fmin', type=float, default=1e9)
+    ap.add_argument('--fmax', type=float, default=6e9)
+    ap.add_argument('--slots', type=int, default=6)
+    ap.add_argument('--fp64', type=int, default=None, help='FP64 solves to time and compare (default: all)')
+    ap.add_argument('--dmax', type=float, default=0.2e-3)
+    ap.add_argument('--no-sequential-mixed', action='store_true')
+    a = ap.parse_args()
+    import torch
+    from .board import stub_filter_board
+    torch.cuda.set_device(0)
+    bd = stub_filter_board(dmax=a.dmax)
+    out = run(bd, np.linspace(a.fmin, a.fmax, a.freqs), slots=a.slots, fp64_count=a.fp64,
+              sequential_mixed=not a.no_sequential_mixed)
+    print(json.dumps(out))
+
+
+if __name__ == '__main__':
+    main()
