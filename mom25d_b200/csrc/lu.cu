@@ -1446,13 +1446,14 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             Gp = std::min(gcap, std::max(Gp, (n - k0 + rows_cap - 1) / rows_cap));
             const int cs = (n - k0 + Gp - 1) / Gp;
             const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
-            M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), H));
             void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
-            if (psmem <= (size_t)smem_cap)
+            if (psmem <= (size_t)smem_cap) {                           // (flagged records: no barrier to reset)
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R>, dim3(Gp), dim3(PANEL_THREADS), args,
                                                       psmem, H));
-            else
+            } else {
+                M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), H));
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, H));
+            }
             m25_note_launch();
             if ((rc = laswp(k0, jb, K0, k0, H))) return rc;                // left, inside the outer panel
             if ((rc = laswp(k0, jb, k0 + jb, KE, H))) return rc;           // the rest of the outer panel
