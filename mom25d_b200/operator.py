@@ -34,7 +34,7 @@ c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
 MIXED_MAX_ITER = 30          # fast.py:255
 FRESH_STALL = (4, 0.1)       # fast.py:256
 MIXED_RTOL = 1e-6            # fast.py:366 (FastOperator.mixed_tol)
-PREDICT_AFTER = 6            # iterations after which a fresh factor's refinement may be judged hopeless (gmres_batched)
+PREDICT_AFTER = 6            # iterations after which a fresh factor's refinement may be given up as hopeless (gmres_batched)
 MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
 REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
 REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most

@@ -3,7 +3,7 @@ mom25d_b200.serve - (board, frequency) solves served as they arrive, several at 
 
     python -m mom25d_b200.serve [--rate 20] [--requests 40] [--slots 4] [--seed 0]
 
-The north-star serving mode of the hot path (the reference solves one board's sweep at a time, sim.py:331 /
+The serving mode of the hot path (the reference solves one board's sweep at a time, sim.py:331 /
 run.py:41; this is the request loop a service puts in front of it):
 
   - boards stay resident: each board's mesh, near-pair lists and device geometry are built on its first request
