@@ -215,6 +215,11 @@ int m25_near_spmm_rows(const m25_mesh *g, const long long *d_off, const int *d_Q
 /* Z (complex64, ld) += vv at (ri, ci): the near field into the mixed-precision matrix. */
 int m25_coo_add_c64(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, float *d_Z, long ld,
                     void *stream);
+/* Z (row-major n x n, leading dimension ld; complex64 when single, else complex128) += vv (complex128) at the
+ * distinct entries (ri, ci): the lumped elements and conductor loss of the reference's extra_blocks
+ * (fast.py:628-641), added into the filled Z. An index outside [0, n) is reported by m25_sync_check. */
+int m25_coo_add(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, void *d_Z, long ld, int n, int single,
+                void *stream);
 /* Y = Z X for a resident double Z (row-major n x n, leading dimension ld) and X (n x k, k <= 16): the dense
  * products of the refinement when the double Z stays on the device (fast.py:1009, _solve_kept: A = Z @ V). */
 int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double *d_X, int k, double *d_Y, void *stream);

@@ -237,17 +237,20 @@ def _on_copper(rects, x, y, tol=1e-9):
     return any(x0 - tol <= x <= x1 + tol and y0 - tol <= y <= y1 + tol for x0, y0, x1, y1 in rects)
 
 
-def mesh_layers(stack, shapes, dmax, ncross=6, grade=1.0, w_ref=None, vias=(), pieces=None):
+def mesh_layers(stack, shapes, dmax, ncross=6, grade=1.0, w_ref=None, vias=(), pieces=None, lines=None):
     """The meshes of every interface of `shapes` ({interface: [rects]}) by tensor_mesh, concatenated in interface
     order. pieces ({interface: [[rects], ...]}): mesh each group of rectangles on its own (disjoint traces).
     Via axes on an interface become grid lines there, so each via has a mesh vertex on every interface it
-    attaches to. Returns (nodes, tris, tri_layer)."""
+    attaches to; lines ({interface: (xs, ys)}) adds grid lines (a lumped element's cut line).
+    Returns (nodes, tris, tri_layer)."""
     nodes, tris, tl, off = [], [], [], 0
     for k in sorted(shapes):
         groups = (pieces or {}).get(k) or [shapes[k]]
         for rects in groups:
             vx = [v.x for v in vias if v.k_bot <= k <= v.k_top and _on_copper(rects, v.x, v.y)]
             vy = [v.y for v in vias if v.k_bot <= k <= v.k_top and _on_copper(rects, v.x, v.y)]
+            lx, ly = (lines or {}).get(k, ((), ()))
+            vx, vy = vx + list(lx), vy + list(ly)
             wr = w_ref.get(k) if isinstance(w_ref, dict) else w_ref
             nd, tr = tensor_mesh(rects, dmax, ncross, 1.01 * max(wr or 0, 1.5 * dmax), vx, vy, grade=grade)
             nodes.append(nd)

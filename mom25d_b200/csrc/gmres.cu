@@ -362,6 +362,40 @@ extern "C" int m25_coo_add_c64(const int *d_ri, const int *d_ci, const double *d
     return M25_OK;
 }
 
+int *m25_dev_err_word();
+
+// Z (row-major, ld) += vv at (ri, ci), every (ri, ci) distinct (no atomics: one thread an entry), complex128 or
+// complex64 (rounded on store)
+template <typename R>
+__global__ void k_coo_add_unique(const int *ri, const int *ci, const double *vv, long nnz, R *Z, long ld, long n,
+                                 int *err)
+{
+    const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const long r = ri[e], c = ci[e];
+    if (r < 0 || r >= n || c < 0 || c >= n) { dev_error(err, M25_DEV_INDEX); return; }
+    const size_t o = 2 * ((size_t)r * ld + c);
+    Z[o] = (R)((double)Z[o] + vv[2 * e]);
+    Z[o + 1] = (R)((double)Z[o + 1] + vv[2 * e + 1]);
+}
+
+extern "C" int m25_coo_add(const int *d_ri, const int *d_ci, const double *d_vv, long nnz, void *d_Z, long ld,
+                           int n, int single, void *stream)
+{
+    M25_REQUIRE(nnz >= 0 && (!nnz || (d_ri && d_ci && d_vv && d_Z)) && n >= 0 && ld >= n,
+                "m25_coo_add: ri, ci, vv, Z, nnz >= 0, ld >= n");
+    if (!nnz) return M25_OK;
+    int *err = m25_dev_err_word();
+    if (single)
+        k_coo_add_unique<float><<<(nnz + 255) / 256, 256, 0, S(stream)>>>(d_ri, d_ci, d_vv, nnz, (float *)d_Z, ld,
+                                                                            n, err);
+    else
+        k_coo_add_unique<double><<<(nnz + 255) / 256, 256, 0, S(stream)>>>(d_ri, d_ci, d_vv, nnz, (double *)d_Z,
+                                                                             ld, n, err);
+    M25_LAUNCH_CHECK("k_coo_add_unique");
+    return M25_OK;
+}
+
 extern "C" int m25_border_mv(const double *d_B, const double *d_C, int Ne, int Nv, const double *d_X, int k,
                              double *d_Y, void *stream)
 {

@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import P, check, lib, stream_ptr
+from ._lib import M25Error, P, check, lib, stream_ptr
 from .device import DeviceGeometry, DeviceTables, DeviceVias
 
 c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
@@ -64,6 +64,7 @@ class DirectSolver:
         self.last_path = None
         self.last_lu_ms = self.last_lu_c64_ms = None
         self.attempts = []                 # reused-LU attempts: (f, f0, cap, iterations, converged, residual)
+        self.extras = None                 # extras.ExtraBlocks: lumped elements, conductor loss (fast.py:628-641)
 
     # ---- buffers kept across frequencies ---------------------------------------------------------------------------
     def _buf(self, name, shape, dtype):
@@ -113,6 +114,8 @@ class DirectSolver:
             t0 = time.perf_counter()
             self.vias.assemble(Z, N, qcorr)
             self._t('vias', t0)
+            if self.extras is not None:                   # lumped elements, conductor loss (fast.py:628-641)
+                self.extras.add(Z, f, s)
             return Z
         Z = self._buf('Z64', (N, N), torch.complex64)
         check(lib().m25_fill_far(P(Z), c_long(N), c_int(1), ctypes.byref(dg.mesh), None, ctypes.byref(tb.tables32),
@@ -133,6 +136,8 @@ class DirectSolver:
         t0 = time.perf_counter()
         self.vias.assemble(None, N, qcorr, Z64=Z, B=self.Bv, C=self.Cv)
         self._t('vias', t0)
+        if self.extras is not None:
+            self.extras.add(Z, f, s)
         return Z
 
     # ---- the exact double-precision operator (fast.py:571-593) --------------------------------------------------------
@@ -235,6 +240,9 @@ class DirectSolver:
             precision = 'double'                          # fast.py:740: near a failure, double
         if precision == 'mixed' and self._hybrid_fits():
             return self._solve_kept(f, E)
+        if precision == 'mixed' and self.extras is not None:
+            raise M25Error("lumped elements / conductor loss: the matrix-free refinement operator does not carry "
+                           "them; solve this size in double precision (precision='double')")
         self.last_path = precision
         single = precision == 'mixed'
         t0 = time.perf_counter()

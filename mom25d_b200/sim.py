@@ -45,12 +45,23 @@ class Simulation:
     {interface: [rects]}, or Simulation.from_board(board)."""
 
     def __init__(self, stack=None, shapes=None, ports=(), vias=(), dmax=0.3e-3, w_ref=None, ncross=6, grade=1.0,
-                 near_fac=5.0, solver='direct', precision='auto', gpu='auto', verbose=False, board=None, tf32=None):
+                 near_fac=5.0, solver='direct', precision='auto', gpu='auto', verbose=False, board=None, tf32=None,
+                 lumped=(), metal=None):
+        # lumped (extras.SeriesLumped) and metal (extras.Metal): the reference's sim.py:331-333 arguments, added
+        # into Z as fast.py:628-641 does; a lumped element's cut line becomes a mesh line (sim.py:438)
         if board is None:
             if stack is None or shapes is None:
                 raise ValueError("Simulation needs (stack, shapes) or board=")
             vias = list(vias) + [p.via for p in ports if isinstance(p, ViaPort) and p.via not in vias]
-            nodes, tris, tl = mesh_layers(stack, shapes, dmax, ncross=ncross, grade=grade, w_ref=w_ref, vias=vias)
+            lines = {}
+            for el in lumped:                             # along x: the cut is the line x = c.x; along y: y = c.y
+                xl, yl = lines.setdefault(el.layer, ([], []))
+                if abs(el.lp.d[0]) >= abs(el.lp.d[1]):
+                    xl.append(float(el.lp.c[0]))
+                else:
+                    yl.append(float(el.lp.c[1]))
+            nodes, tris, tl = mesh_layers(stack, shapes, dmax, ncross=ncross, grade=grade, w_ref=w_ref, vias=vias,
+                                          lines=lines)
             board = Board(stack, nodes, tris, tl, list(vias), list(ports), dmax, near_fac, 'simulation',
                           {k: list(v) for k, v in shapes.items()})
         if solver != 'direct':
@@ -67,6 +78,10 @@ class Simulation:
             from . import umma_available
             tf32 = umma_available()
         self.fast = DirectSolver(self.geo, tf32=tf32)
+        self.lumped, self.metal = list(lumped), metal
+        if self.lumped or metal is not None:
+            from .extras import ExtraBlocks
+            self.fast.extras = ExtraBlocks(self.geo, self.lumped, metal)
         self.solver = 'direct'
         self.log.record('setup', time.perf_counter() - t, f"N={self.N}, {self.fast.dg.npairs} near pairs")
 
