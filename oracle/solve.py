@@ -161,3 +161,131 @@ class Direct:
     def sparams(self, f, precision='double'):
         X, info = self.solve(f, precision=precision)
         return self.geo.sparams_from_currents(X), X, info
+
+
+MIXED_RETRY = 1.25        # fast.py:252-253
+REUSE_ITER = (8, 60)      # fast.py:260
+REUSE_KEEP = 4            # fast.py:262
+
+
+class KeptSweep:
+    """The reference's CPU mixed path at sizes where a double Z fits in host memory (fast.py:704-850 with no GPU:
+    `dense_kept`, then _solve_kept, fast.py:996-1084): Z filled in double (the compiled core's fill_far and
+    near_into_dense, the via blocks), equilibrated; batched GMRES on the dense double Z (A = Z @ V) preconditioned
+    by the complex64 LU (LAPACK cgetrf through SciPy) kept from the nearest frequency within the learnt reach
+    (fast.py:974-994), capped at what a fresh one costs; else a fresh complex64 LU of Z, kept (up to keep_max);
+    else the double LU of the same Z, and double up to MIXED_RETRY x f (fast.py:740-744, 1075-1084).
+    core: the reference's compiled core (oracle/_ref) or this package's C restatement; same names either way."""
+
+    def __init__(self, geo, core=None, keep_max=REUSE_KEEP, mixed_tol=1e-6):
+        self.geo = geo
+        self.core = core
+        self.direct = Direct(geo)
+        self.kept, self.reach, self.t_iter, self.mixed_failed = [], float(np.log(2.0)), None, 0.0
+        self.keep_max, self.mixed_tol = keep_max, mixed_tol
+        self.iters, self.last_path, self.timings = [], None, {}
+
+    def _tick(self, name, t0):
+        import time
+        self.timings[name] = self.timings.get(name, 0.0) + time.perf_counter() - t0
+        return time.perf_counter()
+
+    def impedance(self, f):
+        """Z at f as the reference's dense path builds it (fast.py:770-790), the compiled core where given."""
+        import time
+        d, geo = self.direct, self.geo
+        t = time.perf_counter()
+        d.setup(f)
+        t = self._tick('tables', t)
+        Z = np.zeros((geo.N, geo.N), complex)
+        c = self.core
+        (c.fill_far if c is not None else fill_far)(Z, geo.g, d.tb, d.w)
+        t = self._tick('fill_far', t)
+        d.qcorr = (c.near_into_dense if c is not None else near_into_dense)(Z, geo.g, d.tb, d.q, d.nP32, d.nQ32, d.w)
+        d.q['stat_ready'] = True
+        t = self._tick('near', t)
+        if geo.Nv:
+            QF = fan_columns(geo, geo.g, d.tb, d.nP, d.nQ, d.qcorr)
+            d.B, d.C, d.vk = via_blocks(geo, f, QF)
+            Ne = geo.Ne
+            Z[:Ne, Ne:], Z[Ne:, :Ne], Z[Ne:, Ne:] = d.B, d.B.T, d.C
+        self._tick('vias', t)
+        return Z
+
+    def _reusable(self, f):
+        if not self.kept:
+            return None
+        k = min(self.kept, key=lambda k: abs(np.log(f / k[0])))
+        return k if abs(np.log(f / k[0])) <= self.reach else None
+
+    def _drop_kept(self):
+        lf = np.log([k[0] for k in self.kept])
+        gap = [min((abs(lf[i] - y) for j, y in enumerate(lf) if j != i), default=0.0) for i in range(len(lf))]
+        del self.kept[int(np.argmin(gap))]
+
+    def _refine(self, A, B, M, restart):
+        Y, self.iters = gmres_batched(A, B, M=M, rtol=self.mixed_tol, restart=restart, maxiter=1)
+        rel = np.linalg.norm(B - A(Y), axis=0) / np.maximum(np.linalg.norm(B, axis=0), 1e-300)
+        return Y, bool((rel <= 100 * self.mixed_tol).all()), float(rel.max())
+
+    def solve(self, f, E=None, precision='mixed'):
+        """Currents at f for the excitation E (default: the ports'); precision 'mixed' (the reference's default
+        above 3,500 unknowns, sim.py:61) or 'double'."""
+        return self.solve_z(f, self.impedance(f), E, precision)
+
+    def solve_z(self, f, Z, E=None, precision='mixed'):
+        """solve() with Z at f already built (self.impedance(f)); Z is equilibrated and overwritten."""
+        import time
+        geo = self.geo
+        E = geo.excitation() if E is None else E
+        t = time.perf_counter()
+        dsc = 1.0 / np.sqrt(np.abs(np.diagonal(Z)).astype(float) + 1e-300)
+        equilibrate(Z, dsc)
+        B = dsc[:, None] * E
+        t = self._tick('equilibrate', t)
+        if precision == 'mixed' and f <= MIXED_RETRY * self.mixed_failed:
+            precision = 'double'
+        if precision == 'double':
+            F = lu(Z)
+            t = self._tick('lu', t)
+            X = dsc[:, None] * lu_solve(F, B)
+            self._tick('solve', t)
+            self.last_path = 'double'
+            return X
+        A = lambda V: Z @ V
+        k = self._reusable(f)
+        if k is not None:
+            f0, F0, d0, t_fresh = k
+            r = (d0 / dsc)[:, None]
+            cap = int(np.clip(0.8 * t_fresh / max(self.t_iter or 1e-3, 1e-6), *REUSE_ITER))
+            t1 = time.perf_counter()
+            Y, ok, rel = self._refine(A, B, lambda R: r * lu_solve(F0, r * R), cap)
+            self.t_iter = (time.perf_counter() - t1) / max(1, max(self.iters, default=1))
+            d = abs(np.log(f / f0))
+            if ok and max(self.iters) <= cap // 2:
+                self.reach = max(self.reach, 1.25 * d)
+            elif not ok:
+                self.reach = min(self.reach, 0.8 * d)
+            t = self._tick('refine', t)
+            if ok:
+                self.last_path = 'reused'
+                return dsc[:, None] * Y
+        t0 = time.perf_counter()
+        F = lu(Z.astype(np.complex64))
+        t = self._tick('lu', t)
+        t1 = time.perf_counter()
+        Y, ok, rel = self._refine(A, B, lambda R: lu_solve(F, R), MIXED_MAX_ITER)
+        self.t_iter = (time.perf_counter() - t1) / max(1, max(self.iters, default=1))
+        t = self._tick('refine', t)
+        if ok:
+            self.kept.append((f, F, dsc, time.perf_counter() - t0))
+            while len(self.kept) > self.keep_max:
+                self._drop_kept()
+            self.last_path = 'fresh'
+            return dsc[:, None] * Y
+        del F
+        self.mixed_failed = max(self.mixed_failed, f)
+        self.last_path = 'double (after mixed)'
+        X = dsc[:, None] * lu_solve(lu(Z), B)
+        self._tick('lu', t)
+        return X
