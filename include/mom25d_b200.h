@@ -200,6 +200,11 @@ int m25_axpy_cols(double *d_W, const double *d_V, const double *d_a, long N, int
  * W -= sum_i V_i h[i, c] (h complex128[nv * k]). */
 int m25_dotc_multi(const double *d_V, int nv, long N, int k, const double *d_W, double *d_out, void *stream);
 int m25_axpy_multi(double *d_W, const double *d_V, int nv, long N, int k, const double *d_h, void *stream);
+/* One Arnoldi step of the batched GMRES (replaces the per-vector modified Gram-Schmidt loop of gmres_batched,
+ * fast.py:1470-1476) without a host round trip: W orthogonalised against the basis blocks V_0 .. V_j (classical
+ * Gram-Schmidt applied twice) and normalised into V_{j+1} = d_V + (j + 1) N k complex; the Hessenberg column
+ * (j + 1 projections, then the norm as a real) into d_h ((j + 2) x k complex128). d_tmp: (j + 1) x k complex128. */
+int m25_arnoldi_orth(double *d_V, int j, long N, int k, double *d_W, double *d_h, double *d_tmp, void *stream);
 /* Y[n, c] = X[n, c] s[c] (times rows[n] when d_rows != NULL); s complex128[k] or NULL for 1. */
 int m25_scale_cols(double *d_Y, const double *d_X, const double *d_s, const double *d_rows, long N, int k,
                    void *stream);
@@ -271,6 +276,11 @@ int m25_umma_available(void);
 int m25_bessel_jn_complex(int order, const double *d_z, long count, double *d_out, void *stream);
 /* Synchronises stream and turns a pending kernel error (or a device-side check, M25_EDEVICE) into a status. */
 int m25_sync_check(void *stream);
+/* Exercises the failure-detection path (no counterpart in the reference, whose CPU and Vulkan paths have no device
+ * waits): the cooperative kernels' bounded grid barrier entered by one block that waits for a block never
+ * launched. The wait gives up at its iteration limit (a few seconds), the kernel returns, and the next
+ * m25_sync_check reports M25_EDEVICE (M25_DEV_TIMEOUT) with the context still usable. */
+int m25_wait_selftest(void *stream);
 /* How many kernels this library has launched in the process (a counter for measurements). */
 long long m25_launch_count(void);
 

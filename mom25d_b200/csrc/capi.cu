@@ -61,21 +61,24 @@ extern "C" int m25_device_info(int *sm_count, size_t *free_bytes, size_t *total_
     return M25_OK;
 }
 
-// Synchronises the stream and reads (then clears) the device error word: M25_EDEVICE with the code if a kernel
-// reported one (an index out of range, a bounded wait that gave up, a zero pivot).
+// Synchronises the stream and reads (then clears) the device error words: M25_EDEVICE with the code if a kernel
+// reported one (an index out of range, a bounded wait that gave up, a zero pivot). Two words per device: the
+// library's, and m25_getrs_noalloc's own where that has run. Both are read and both are cleared, so that a code
+// left in one cannot make a later call fail; the first nonzero code is the one reported.
 extern "C" int m25_sync_check(void *stream)
 {
     cudaStream_t s = (cudaStream_t)stream;
     M25_CHECK(cudaStreamSynchronize(s));
     int *w = m25_dev_err_word();
     if (!w) { g_err = "m25_sync_check: no device error word"; return M25_ECUDA; }
-    int code = 0;
+    int code = 0, code2 = 0;
     M25_CHECK(cudaMemcpy(&code, w, sizeof(int), cudaMemcpyDeviceToHost));
     int *nw = m25_noalloc_status_word();               // m25_getrs_noalloc's own word, where it has run
-    if (!code && nw) {
-        M25_CHECK(cudaMemcpy(&code, nw, sizeof(int), cudaMemcpyDeviceToHost));
-        if (code) w = nw;
+    if (nw) {
+        M25_CHECK(cudaMemcpy(&code2, nw, sizeof(int), cudaMemcpyDeviceToHost));
+        if (code2) M25_CHECK(cudaMemset(nw, 0, sizeof(int)));
     }
+    if (!code) code = code2;
     if (code) {
         M25_CHECK(cudaMemset(w, 0, sizeof(int)));
         char buf[128];
@@ -85,5 +88,28 @@ extern "C" int m25_sync_check(void *stream)
         g_err = buf;
         return M25_EDEVICE;
     }
+    return M25_OK;
+}
+
+// ---- failure detection without a fault: a bounded wait that runs out ------------------------------------------------
+// The grid barrier of the cooperative kernels (grid_sync), entered by one block that waits for a second block which
+// is never launched: the wait ends at its iteration limit, the device error word gets M25_DEV_TIMEOUT and the
+// kernel returns. m25_sync_check then reports M25_EDEVICE and the context stays usable.
+static __device__ unsigned g_selftest_barrier[2];
+
+__global__ void k_wait_selftest(int *err)
+{
+    if (threadIdx.x == 0) { g_selftest_barrier[0] = 0u; g_selftest_barrier[1] = 0u; }
+    GridBarrier b{&g_selftest_barrier[0], &g_selftest_barrier[1]};
+    unsigned phase = 0;
+    grid_sync(b, 2u, phase, err);
+}
+
+extern "C" int m25_wait_selftest(void *stream)
+{
+    int *err = m25_dev_err_word();
+    if (!err) { g_err = "m25_wait_selftest: no device error word"; return M25_ECUDA; }
+    k_wait_selftest<<<1, 32, 0, (cudaStream_t)stream>>>(err);
+    M25_LAUNCH_CHECK("k_wait_selftest");
     return M25_OK;
 }

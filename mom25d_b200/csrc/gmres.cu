@@ -438,3 +438,69 @@ extern "C" int m25_axpy_multi(double *d_W, const double *d_V, int nv, long N, in
     M25_LAUNCH_CHECK("k_axpy_multi");
     return M25_OK;
 }
+
+// ---- one Arnoldi step of the batched GMRES on the device ------------------------------------------------------------
+// h[i, c] += d[i, c] (n complex coefficients): the second Gram-Schmidt pass's correction
+__global__ void k_add_coef(double *h, const double *d, int n)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    h[2 * e] += d[2 * e];
+    h[2 * e + 1] += d[2 * e + 1];
+}
+
+// V[n, c] = W[n, c] / sqrt(re nrm2[c]) (a zero norm: V = 0, the column has broken down and stays converged)
+__global__ void k_scale_rnorm(double *V, const double *W, const double *nrm2, long N, int k)
+{
+    const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= N * k) return;
+    const double s = nrm2[2 * (e % k)];
+    const double r = s > 0 ? rsqrt(s) : 0.0;
+    zd w = ldc<double>(W, e);
+    stc<double>(V, e, w * r);
+}
+
+// nrm2[c] = (sqrt(re nrm2[c]), 0): the subdiagonal entry of the Hessenberg column
+__global__ void k_sqrt_norms(double *nrm2, int k)
+{
+    const int c = threadIdx.x;
+    if (c >= k) return;
+    nrm2[2 * c] = sqrt(fmax(nrm2[2 * c], 0.0));
+    nrm2[2 * c + 1] = 0.0;
+}
+
+// W (the operator applied to the j-th preconditioned direction) orthogonalised against the basis blocks
+// V_0 .. V_j by classical Gram-Schmidt applied twice, and normalised into V_{j+1}; the Hessenberg column goes to
+// h ((j + 2) x k complex: the j + 1 projections, then the norm). tmp: (j + 1) x k complex of scratch. Nothing
+// is read back: the host takes h once per step.
+extern "C" int m25_arnoldi_orth(double *d_V, int j, long N, int k, double *d_W, double *d_h, double *d_tmp,
+                                void *stream)
+{
+    M25_REQUIRE(d_V && d_W && d_h && d_tmp && j >= 0 && j < 65535 && k >= 1 && k <= 16 && N >= 1,
+                "m25_arnoldi_orth: V, W, h, tmp, 0 <= j, 1 to 16 columns");
+    cudaStream_t s = S(stream);
+    const int nv = j + 1;
+    const size_t hb = sizeof(double) * 2 * (size_t)nv * k;
+    dim3 grid((unsigned)std::min<long>(148, (N + 255) / 256), (unsigned)nv);
+    const long t = N * k;
+    M25_CHECK(cudaMemsetAsync(d_h, 0, hb + sizeof(double) * 2 * k, s));
+    k_dotc_multi<<<grid, 256, 0, s>>>(d_V, N, k, d_W, d_h);
+    M25_LAUNCH_CHECK("k_dotc_multi");
+    k_axpy_multi<<<(t + 255) / 256, 256, 0, s>>>(d_W, d_V, nv, N, k, d_h);
+    M25_LAUNCH_CHECK("k_axpy_multi");
+    M25_CHECK(cudaMemsetAsync(d_tmp, 0, hb, s));
+    k_dotc_multi<<<grid, 256, 0, s>>>(d_V, N, k, d_W, d_tmp);
+    M25_LAUNCH_CHECK("k_dotc_multi");
+    k_axpy_multi<<<(t + 255) / 256, 256, 0, s>>>(d_W, d_V, nv, N, k, d_tmp);
+    M25_LAUNCH_CHECK("k_axpy_multi");
+    k_add_coef<<<(nv * k + 255) / 256, 256, 0, s>>>(d_h, d_tmp, nv * k);
+    M25_LAUNCH_CHECK("k_add_coef");
+    double *nrm = d_h + 2 * (size_t)nv * k;
+    k_dotc_cols<<<(int)std::min<long>(592, (N + 255) / 256), 256, 0, s>>>(d_W, d_W, N, k, nrm);
+    M25_LAUNCH_CHECK("k_dotc_cols");
+    k_scale_rnorm<<<(t + 255) / 256, 256, 0, s>>>(d_V + 2 * (size_t)nv * N * k, d_W, nrm, N, k);
+    M25_LAUNCH_CHECK("k_scale_rnorm");
+    k_sqrt_norms<<<1, 32, 0, s>>>(nrm, k);
+    M25_LAUNCH_CHECK("k_sqrt_norms");
+    return M25_OK;
+}

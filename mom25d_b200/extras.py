@@ -19,70 +19,114 @@ MU0 = 4e-7 * np.pi
 
 
 def rlc(R=0.0, L=0.0, C=None, parallel=False):
-    """The impedance function of a series (default) or parallel R-L-C element (sim.py:48-56)."""
-    def Z(f):
-        w = 2 * np.pi * f
-        if not parallel:
-            return R + 1j * w * L + (1 / (1j * w * C) if C else 0)
-        return 1 / ((1 / R if R else 0) + (1 / (1j * w * L) if L else 0) + (1j * w * C if C else 0))
+    """Z(f) of an R-L-C element, the reference's rlc (sim.py:51-58) by its definition: in series the branch
+    impedances R, j w L and 1 / (j w C) add (no C: no capacitor in the string); in parallel their admittances
+    add, a zero R or L or a missing C being an absent branch."""
+    if parallel:
+        def Z(f):
+            jw = 2j * np.pi * f
+            y = 0.0
+            if R:
+                y += 1.0 / R
+            if L:
+                y += 1.0 / (jw * L)
+            if C:
+                y += jw * C
+            return 1.0 / y
+    else:
+        def Z(f):
+            jw = 2j * np.pi * f
+            z = R + jw * L
+            return z + 1.0 / (jw * C) if C else z
     return Z
 
 
-def _zfun(Z):
-    return Z if callable(Z) else (lambda f, Z=Z: complex(Z))
+def as_impedance(Z):
+    """An impedance given as ohms or as a function of f, as a function of f."""
+    if callable(Z):
+        return Z
+    z = complex(Z)
+    return lambda f: z
 
 
 class SeriesLumped:
     """A series element across a strip (sim.py:221-226): the cut line of `width` at `center`, transverse to
-    `direction`, on interface `layer`; Z an impedance (ohm) or a function of f (e.g. rlc(...))."""
+    `direction`, on interface `layer`; Z an impedance (ohm) or a function of f (e.g. rlc(...)). The reference's
+    own SeriesLumped objects work here as well (the same .lp cut line and .Z)."""
 
     def __init__(self, layer, center, direction, width, Z, name=''):
         from .board import GapPort
         self.lp = GapPort(layer, center, direction, width, 0.0, name)   # the cut line's geometry
-        self.layer, self.Z, self.name = int(layer), _zfun(Z), name
+        self.layer, self.Z, self.name = int(layer), as_impedance(Z), name
+
+
+def _skin_wavenumber(w, sigma):
+    """(1 + j) / delta, delta = sqrt(2 / (w mu0 sigma)) the skin depth of a good conductor at angular frequency w."""
+    return (1.0 + 1.0j) * np.sqrt(0.5 * w * MU0 * sigma)
+
+
+def _slab_impedance(w, sigma, t):
+    """The surface impedance of a conductor slab of thickness t seen from one face: Zc coth(gamma t) with the
+    wave impedance Zc = gamma / sigma of the conductor (tends to 1 / (sigma t) at DC)."""
+    gm = _skin_wavenumber(w, sigma)
+    return (gm / sigma) / np.tanh(gm * t)
+
+
+def _through_layer(z_load, w, sigma, t):
+    """The impedance at the outer face of a finish layer (sigma, t) backed by z_load: the layer as a line section
+    of wave impedance Zc = gamma / sigma and electrical length gamma t terminated in z_load."""
+    gm = _skin_wavenumber(w, sigma)
+    zc, th = gm / sigma, np.tanh(gm * t)
+    return zc * (z_load + zc * th) / (zc + z_load * th)
 
 
 class Metal:
-    """Conductor loss (sim.py:228-270): Zs = (g / sigma) coth(g t), g = (1 + j) / delta; rough (m RMS) scales its
-    real part by Hammerstad and Jensen's 1 + 2/pi atan(1.4 (rough / delta)^2); finish [(sigma, t), ...] (outermost
-    first) on the interfaces of `on` ({interface: share}) multiplies Zs there by 1 + share (F - 1), F the finished
-    face's impedance over the bare one's."""
+    """Conductor loss of the strips (the reference's Metal, sim.py:228-270): the surface impedance Zs of a copper
+    slab (sigma, t), its resistance scaled by Hammerstad and Jensen's roughness factor for an RMS roughness
+    `rough`, and where a surface finish ([(sigma, t), ...], outermost first) covers the interfaces of `on`
+    ({interface: share}), Zs there scaled by 1 + share (F - 1), F the finished face over the bare face. The
+    reference's own Metal objects work here as well (the same zs_edges)."""
 
     def __init__(self, sigma=5.8e7, t=35e-6, rough=0.0, finish=(), on=None):
         self.sigma, self.t, self.rough = sigma, t, rough
         self.finish, self.on = [tuple(x) for x in finish], dict(on or {})
 
-    def zs(self, f, k=None):
-        g = (1 + 1j) * np.sqrt(2 * np.pi * f * MU0 * self.sigma / 2)
-        z = g / self.sigma / np.tanh(g * self.t)
-        if self.rough:
-            delta = 1 / np.sqrt(np.pi * f * MU0 * self.sigma)
-            z = z.real * (1 + 2 / np.pi * np.arctan(1.4 * (self.rough / delta) ** 2)) + 1j * z.imag
-        share = self.on.get(k, 0.0) if self.finish else 0.0
-        if share:
-            z = z * (1 + share * (self.face_factor(f) - 1))
-        return z
+    def roughness_factor(self, f):
+        """1 + (2 / pi) atan(1.4 (rough / delta)^2), delta the copper's skin depth at f (1 when smooth)."""
+        if not self.rough:
+            return 1.0
+        delta = np.sqrt(1.0 / (np.pi * f * MU0 * self.sigma))
+        return 1.0 + (2.0 / np.pi) * np.arctan(1.4 * (self.rough / delta) ** 2)
 
     def face_factor(self, f):
-        """The finished face's impedance over the bare copper face's: each finish layer a line section
-        Z_i = g_i / sigma_i loading the one beneath, from the copper outwards."""
+        """The finished face's impedance over the bare copper face's at f: the finish layers stacked on the
+        copper slab from the innermost outwards."""
         w = 2 * np.pi * f
-        gam = lambda s: (1 + 1j) * np.sqrt(w * MU0 * s / 2)
-        bare = gam(self.sigma) / self.sigma / np.tanh(gam(self.sigma) * self.t)
+        bare = _slab_impedance(w, self.sigma, self.t)
         z = bare
-        for s, tl in reversed(self.finish):
-            zc, th = gam(s) / s, np.tanh(gam(s) * tl)
-            z = zc * (z + zc * th) / (zc + z * th)
+        for sigma, t in self.finish[::-1]:
+            z = _through_layer(z, w, sigma, t)
         return z / bare
 
+    def zs(self, f, k=None):
+        """Zs at f, on interface k (its finish, if any)."""
+        z = _slab_impedance(2 * np.pi * f, self.sigma, self.t)
+        kr = self.roughness_factor(f)
+        if kr != 1.0:
+            z = complex(z.real * kr, z.imag)
+        share = self.on.get(k, 0.0) if self.finish else 0.0
+        if share:
+            z = z * (1.0 + share * (self.face_factor(f) - 1.0))
+        return z
+
     def zs_edges(self, f, edge_layer):
-        """Zs per RWG edge by its interface: one value unless a finish covers some interfaces."""
+        """Zs for every RWG edge by its interface: a scalar when no finish is set on some interfaces."""
         if not (self.finish and self.on):
             return self.zs(f)
-        out = np.full(len(edge_layer), self.zs(f), complex)
-        for k in self.on:
-            out[edge_layer == k] = self.zs(f, k)
-        return out
+        edge_layer = np.asarray(edge_layer)
+        ks = np.unique(edge_layer)
+        per = np.array([self.zs(f, int(k)) if int(k) in self.on else self.zs(f) for k in ks], complex)
+        return per[np.searchsorted(ks, edge_layer)]
 
 
 def gram_matrix(rwg, P3, W3):
@@ -179,17 +223,38 @@ class ExtraBlocks:
         S[self.ri, self.ci] = self.values(f)
         return S
 
-    def add(self, Z, f, stream_ptr):
-        """Z (a device complex128 or complex64 N x N tensor, row-major) += S at f, on the stream."""
+    def _device_values(self, f, stream):
+        """The pattern (ri, ci) and S's values at f as device tensors, uploaded on `stream` (a torch stream, or
+        None for the current one) so that the caching allocator hands their memory on only after that stream has
+        used them; the values are kept for the frequency until another is asked for."""
         import torch
-        from ._lib import P, check, lib
+        st = stream if stream is not None else torch.cuda.current_stream()
+        with torch.cuda.stream(st):
+            if self._dev is None:
+                self._dev = (torch.from_numpy(self.ri).to('cuda'), torch.from_numpy(self.ci).to('cuda'))
+            if getattr(self, '_vals_f', None) != f:
+                self._vals = torch.from_numpy(self.values(f)).to('cuda')
+                self._vals_f = f
+        return self._dev[0], self._dev[1], self._vals
+
+    def add(self, Z, f, stream=None):
+        """Z (a device complex128 or complex64 N x N tensor, row-major) += S at f, on the stream (a torch stream,
+        or None for the current one)."""
+        import torch
+        from ._lib import P, check, lib, stream_ptr
         if not self.nnz:
             return
-        if self._dev is None:
-            self._dev = (torch.from_numpy(self.ri).to('cuda'), torch.from_numpy(self.ci).to('cuda'))
-        vv = torch.from_numpy(self.values(f)).to('cuda')
+        ri, ci, vv = self._device_values(f, stream)
         single = int(Z.dtype == torch.complex64)
-        check(lib().m25_coo_add(P(self._dev[0]), P(self._dev[1]), P(vv), ctypes.c_long(self.nnz), P(Z),
-                                ctypes.c_long(Z.shape[1]), ctypes.c_int(Z.shape[0]), single, stream_ptr),
-              'm25_coo_add')
-        self._keep = vv                                       # until the stream has used it
+        check(lib().m25_coo_add(P(ri), P(ci), P(vv), ctypes.c_long(self.nnz), P(Z), ctypes.c_long(Z.shape[1]),
+                                ctypes.c_int(Z.shape[0]), single, stream_ptr(stream)), 'm25_coo_add')
+
+    def apply(self, X, Y, f, stream=None):
+        """Y += S X at f (X, Y device complex128 N x k, contiguous): the extra blocks in the matrix-free
+        refinement operator, as the reference's matvec_exact adds Sx X (fast.py:571-586)."""
+        from ._lib import P, check, lib, stream_ptr
+        if not self.nnz:
+            return
+        ri, ci, vv = self._device_values(f, stream)
+        check(lib().m25_coo_spmm(P(ri), P(ci), P(vv), ctypes.c_long(self.nnz), P(X), ctypes.c_int(X.shape[1]), P(Y),
+                                 stream_ptr(stream)), 'm25_coo_spmm')

@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import M25Error, P, check, lib, stream_ptr
+from ._lib import P, check, lib, stream_ptr
 from .device import DeviceGeometry, DeviceTables, DeviceVias
 
 c_int, c_long, c_double = ctypes.c_int, ctypes.c_long, ctypes.c_double
@@ -82,9 +82,29 @@ class DirectSolver:
     def s(self):
         return stream_ptr(self.stream)
 
-    def _t(self, name, t0):
-        torch.cuda.current_stream().synchronize() if self.stream is None else self.stream.synchronize()
-        self.timings[name] = self.timings.get(name, 0.0) + time.perf_counter() - t0
+    # ---- phase timings: CUDA events on the solver's stream (no host synchronisation on the path) ------------------
+    def _mark(self):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(self.stream if self.stream is not None else torch.cuda.current_stream())
+        return e
+
+    def _t(self, name, e0):
+        """The device time from event e0 (self._mark()) to now is added to phase `name`."""
+        self._pending.append((name, e0, self._mark()))
+
+    @property
+    def timings(self):
+        """Seconds per phase so far (tables, fill, vias, lu, refine, refine_matvec, refine_precond, solve)."""
+        if self._pending:
+            self._pending[-1][2].synchronize()
+            for name, a, b in self._pending:
+                self._timings[name] = self._timings.get(name, 0.0) + a.elapsed_time(b) / 1000.0
+            self._pending = []
+        return self._timings
+
+    @timings.setter
+    def timings(self, value):
+        self._pending, self._timings = [], dict(value)
 
     # ---- tables and fill -----------------------------------------------------------------------------------------
     def setup(self, f, single=False):
@@ -97,10 +117,11 @@ class DirectSolver:
         geo, dg = self.geo, self.dg
         N, Ne = geo.N, geo.Ne
         single = precision == 'mixed'
-        t0 = time.perf_counter()
+        t0 = self._mark()
         self.setup(f, single=single)
         self._t('tables', t0)
         tb, s = self.tabs, self.s
+        t0 = self._mark()
         qcorr = self._buf('qcorr', (max(1, dg.npairs),), torch.complex128)
         if not single:
             Z = self._buf('Z', (N, N), torch.complex128)
@@ -111,11 +132,12 @@ class DirectSolver:
                                  ctypes.byref(dg.quad), P(dg.nP), P(dg.nQ), c_long(dg.npairs), c_double(self.w), s),
                   'm25_near')
             dg.stat_ready = True
-            t0 = time.perf_counter()
+            self._t('fill', t0)
+            t0 = self._mark()
             self.vias.assemble(Z, N, qcorr)
             self._t('vias', t0)
             if self.extras is not None:                   # lumped elements, conductor loss (fast.py:628-641)
-                self.extras.add(Z, f, s)
+                self.extras.add(Z, f, self.stream)
             return Z
         Z = self._buf('Z64', (N, N), torch.complex64)
         check(lib().m25_fill_far(P(Z), c_long(N), c_int(1), ctypes.byref(dg.mesh), None, ctypes.byref(tb.tables32),
@@ -133,11 +155,12 @@ class DirectSolver:
               'm25_coo_add_c64')
         self.Bv = self._buf('Bv', (max(1, Ne * geo.Nv),), torch.complex128)
         self.Cv = self._buf('Cv', (max(1, geo.Nv * geo.Nv),), torch.complex128)
-        t0 = time.perf_counter()
+        self._t('fill', t0)
+        t0 = self._mark()
         self.vias.assemble(None, N, qcorr, Z64=Z, B=self.Bv, C=self.Cv)
         self._t('vias', t0)
         if self.extras is not None:
-            self.extras.add(Z, f, s)
+            self.extras.add(Z, f, self.stream)
         return Z
 
     # ---- the exact double-precision operator (fast.py:571-593) --------------------------------------------------------
@@ -158,6 +181,8 @@ class DirectSolver:
         if geo.Nv:
             check(lib().m25_border_mv(P(self.Bv), P(self.Cv), c_int(Ne), c_int(geo.Nv), P(X), c_int(k), P(Y), s),
                   'm25_border_mv')
+        if self.extras is not None:                       # + S X, the lumped elements and conductor loss
+            self.extras.apply(X, Y, self.f, self.stream)
         return Y
 
     # ---- device vector helpers ------------------------------------------------------------------------------------------
@@ -167,22 +192,11 @@ class DirectSolver:
         check(lib().m25_dotc_cols(P(V), P(W), c_long(V.shape[0]), c_int(k), P(out), self.s), 'm25_dotc_cols')
         return out.cpu().numpy().copy()
 
-    def _dotc_multi(self, Vall, nv, W):
-        """conj(V_i)^T W per column for the first nv basis blocks: (nv, k) complex on the host (one sync)."""
-        N, k = W.shape
-        out = self._buf('dotm', (nv * k,), torch.complex128)
-        check(lib().m25_dotc_multi(P(Vall), c_int(nv), c_long(N), c_int(k), P(W), P(out), self.s), 'm25_dotc_multi')
-        return out.cpu().numpy().reshape(nv, k).copy()
-
     def _axpy_multi(self, W, Vall, nv, h):
         """W -= sum_i V_i h[i] (per column)."""
         N, k = W.shape
         h_d = _lib.dev(np.ascontiguousarray(h, complex))
         check(lib().m25_axpy_multi(P(W), P(Vall), c_int(nv), c_long(N), c_int(k), P(h_d), self.s), 'm25_axpy_multi')
-
-    def _axpy(self, W, V, a):
-        a_d = _lib.dev(np.asarray(a, complex))
-        check(lib().m25_axpy_cols(P(W), P(V), P(a_d), c_long(W.shape[0]), c_int(W.shape[1]), self.s), 'm25_axpy_cols')
 
     def _scale(self, X, s_cols=None, rows=None, out=None):
         Y = torch.empty_like(X) if out is None else out
@@ -193,18 +207,18 @@ class DirectSolver:
 
     # ---- solves -------------------------------------------------------------------------------------------------------
     def _factor(self, Z, single):
+        """LU of Z (double, or complex64 with single=True) in place, and the prepared solve data; the pivots."""
         N = self.geo.N
         ipiv = self._buf('ipiv', (N,), torch.int32)
         work = self._getrf_work(N, single)
-        st = self.stream if self.stream is not None else torch.cuda.current_stream()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(st)
+        a = self._mark()
         check(lib().m25_getrf(P(Z), c_long(N), c_int(N), P(ipiv), c_int(int(single)),
                               c_int(int(single and self.tf32)), P(work), ctypes.c_size_t(work.numel()), self.s),
               'm25_getrf')
-        b.record(st)
+        b = self._mark()
         _lib.sync_check(self.stream, 'm25_getrf')
         self.last_lu_ms = a.elapsed_time(b)                # the factorisation alone, on its stream
+        self._pending.append(('lu', a, b))
         # the solves' diagonal-block inverses and row permutation, once per factor
         nbytes = int(lib().m25_getrs_aux_bytes(c_int(N), c_int(int(single))))
         self.aux = self._buf('getrs_aux_%d' % single, (nbytes,), torch.uint8)
@@ -216,13 +230,7 @@ class DirectSolver:
         """Z^-1 R with the factor (lu_solve(..., trans=1)), R complex128 (N x k) -> complex128."""
         N, k = R.shape
         if single:
-            R64 = torch.empty((N, k), dtype=torch.complex64, device='cuda')
-            check(lib().m25_convert(P(R), c_int(0), P(R64), c_long(N * k), self.s), 'm25_convert')
-            check(lib().m25_getrs_aux(P(Z), c_long(N), c_int(N), c_int(1), P(self.aux), P(R64), c_int(k), self.s),
-                  'm25_getrs_aux')
-            X = torch.empty((N, k), dtype=torch.complex128, device='cuda')
-            check(lib().m25_convert(P(R64), c_int(1), P(X), c_long(N * k), self.s), 'm25_convert')
-            return X
+            return self._solve_c64(dict(Z=Z, aux=self.aux), R)
         X = R.clone()
         check(lib().m25_getrs_aux(P(Z), c_long(N), c_int(N), c_int(0), P(self.aux), P(X), c_int(k), self.s),
               'm25_getrs_aux')
@@ -240,41 +248,26 @@ class DirectSolver:
             precision = 'double'                          # fast.py:740: near a failure, double
         if precision == 'mixed' and self._hybrid_fits():
             return self._solve_kept(f, E)
-        if precision == 'mixed' and self.extras is not None:
-            raise M25Error("lumped elements / conductor loss: the matrix-free refinement operator does not carry "
-                           "them; solve this size in double precision (precision='double')")
         self.last_path = precision
         single = precision == 'mixed'
-        t0 = time.perf_counter()
         Z = self.impedance(f, precision)
-        self._t('fill', t0)
         dsc = self._buf('dsc', (N,), torch.float64)
-        t0 = time.perf_counter()
         if single:
             check(lib().m25_equilibrate_c64(P(Z), c_long(N), c_long(N), P(dsc), self.s), 'm25_equilibrate_c64')
         else:
             check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
         ipiv = self._factor(Z, single)
-        self._t('lu', t0)
-        t0 = time.perf_counter()
+        t0 = self._mark()
         B = self._scale(E, rows=dsc)
         if not single:
             Y = self._lu_solve(Z, ipiv, B, False)
             X = self._scale(Y, rows=dsc)
             self._t('solve', t0)
             return X
-        def A(V):
-            t = time.perf_counter()
-            Y = self._scale(self.matvec_exact(self._scale(V, rows=dsc)), rows=dsc)
-            self._t('refine_matvec', t)
-            return Y
-
-        def M(R):
-            t = time.perf_counter()
-            X = self._lu_solve(Z, ipiv, R, True)
-            self._t('refine_precond', t)
-            return X
-        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, 1, FRESH_STALL)
+        A = lambda V: self._timed('refine_matvec', lambda: self._scale(self.matvec_exact(self._scale(V, rows=dsc)),
+                                                                       rows=dsc))
+        M = lambda R: self._timed('refine_precond', lambda: self._lu_solve(Z, ipiv, R, True))
+        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, FRESH_STALL)
         self._t('refine', t0)
         if not ok:
             raise SolveFailed(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e})")
@@ -325,14 +318,13 @@ class DirectSolver:
         N = self.geo.N
         rec = dict(Z=Z64, ipiv=torch.empty(N, dtype=torch.int32, device='cuda'))
         work = self._getrf_work(N, True)
-        st = self.stream if self.stream is not None else torch.cuda.current_stream()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(st)
+        a = self._mark()
         check(lib().m25_getrf(P(Z64), c_long(N), c_int(N), P(rec['ipiv']), c_int(1), c_int(int(self.tf32)), P(work),
                               ctypes.c_size_t(work.numel()), self.s), 'm25_getrf')
-        b.record(st)
+        b = self._mark()
         _lib.sync_check(self.stream, 'm25_getrf')
         self.last_lu_ms = self.last_lu_c64_ms = a.elapsed_time(b)
+        self._pending.append(('lu', a, b))
         nbytes = int(lib().m25_getrs_aux_bytes(c_int(N), c_int(1)))
         rec['aux'] = torch.empty(nbytes, dtype=torch.uint8, device='cuda')
         check(lib().m25_getrs_prepare(P(Z64), c_long(N), c_int(N), P(rec['ipiv']), c_int(1), P(rec['aux']),
@@ -341,7 +333,7 @@ class DirectSolver:
         return rec
 
     def _solve_c64(self, rec, R):
-        """Z^-1 R with a kept complex64 factor, R complex128 (N x k) -> complex128."""
+        """Z^-1 R with a complex64 factor, R complex128 (N x k) -> complex128."""
         N, k = R.shape
         R64 = torch.empty((N, k), dtype=torch.complex64, device='cuda')
         check(lib().m25_convert(P(R), c_int(0), P(R64), c_long(N * k), self.s), 'm25_convert')
@@ -359,18 +351,17 @@ class DirectSolver:
         for c0 in range(0, k, 16):
             c1 = min(k, c0 + 16)
             Vc = V[:, c0:c1].contiguous() if (c0, c1) != (0, k) else V
-            Yc = torch.empty_like(Vc)
+            Yc = Y if (c0, c1) == (0, k) else torch.empty_like(Vc)
             check(lib().m25_zgemm_skinny(P(Z), c_long(N), c_int(N), P(Vc), c_int(c1 - c0), P(Yc), self.s),
                   'm25_zgemm_skinny')
-            Y[:, c0:c1] = Yc
+            if Yc is not Y:
+                Y[:, c0:c1] = Yc
         return Y
 
     def _solve_kept(self, f, E):
         """fast.py:996-1084 on the device: returns the currents (equilibration undone)."""
-        geo, N = self.geo, self.geo.N
-        t0 = time.perf_counter()
+        N = self.geo.N
         Z = self.impedance(f, 'double')
-        self._t('fill', t0)
         dsc = self._buf('dsc', (N,), torch.float64)
         check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
         dsc = dsc.clone()
@@ -383,14 +374,14 @@ class DirectSolver:
             cap = int(np.clip(0.8 * t_fresh / max(self.t_iter or 1e-3, 1e-6), *REUSE_ITER))
             M = lambda R: self._timed('refine_precond', lambda: self._scale(self._solve_c64(rec, self._scale(R, rows=r)),
                                                                               rows=r))
-            t = time.perf_counter()
-            Y, ok, rel = self.refine(A, B, M, cap, 1)
+            e0, t = self._mark(), time.perf_counter()
+            Y, ok, rel = self.refine(A, B, M, cap)
             self._learn_t_iter((time.perf_counter() - t) / max(1, max(self.iters, default=1)))
             self._reach_learn(abs(np.log(f / f0)), ok, self.iters, cap)
             self.attempts.append(dict(f=f, f0=f0, cap=cap, iters=max(self.iters, default=0), ok=ok, rel=rel))
+            self._t('refine', e0)
             if ok:
                 self.last_path = 'reused'
-                self._t('refine', t)
                 return self._scale(Y, rows=dsc)
         t_fresh0 = time.perf_counter()
         keep_max = self._keep_max()
@@ -398,14 +389,12 @@ class DirectSolver:
             self._drop_kept()                             # room for the new factor
         Z64 = torch.empty((N, N), dtype=torch.complex64, device='cuda')
         check(lib().m25_convert(P(Z), c_int(0), P(Z64), c_long(N * N), self.s), 'm25_convert')
-        t = time.perf_counter()
         rec = self._factor_c64(Z64)
-        self._t('lu', t)
         M = lambda R: self._timed('refine_precond', lambda: self._solve_c64(rec, R))
-        t = time.perf_counter()
-        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, 1, FRESH_STALL, predict=False)
+        e0, t = self._mark(), time.perf_counter()
+        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, FRESH_STALL, predict=False)
         self._learn_t_iter((time.perf_counter() - t) / max(1, max(self.iters, default=1)))
-        self._t('refine', t)
+        self._t('refine', e0)
         if ok:
             self.last_path = 'fresh'
             if keep_max >= 1:
@@ -417,10 +406,10 @@ class DirectSolver:
         self.log.append(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e}): double LU of the "
                         f"same Z, double up to {MIXED_RETRY * f / 1e9:.4g} GHz")
         self.last_path = 'double (after mixed)'
-        t = time.perf_counter()
         ipiv = self._factor(Z, False)
-        self._t('lu', t)
+        t0 = self._mark()
         X = self._lu_solve(Z, ipiv, B, False)
+        self._t('solve', t0)
         return self._scale(X, rows=dsc)
 
     def _learn_t_iter(self, t):
@@ -429,15 +418,16 @@ class DirectSolver:
         self.t_iter = t if self.t_iter is None else min(self.t_iter, t)
 
     def _timed(self, name, fn):
-        t = time.perf_counter()
+        e = self._mark()
         out = fn()
-        self._t(name, t)
+        self._t(name, e)
         return out
 
-    def refine(self, A, B, M, restart, maxiter, stall=None, predict=True):
-        """fast.py:658-663: batched GMRES to MIXED_RTOL; (Y, converged, largest relative residual)."""
-        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, maxiter=maxiter, stall=stall,
-                                           predict=predict)
+    # ---- the refinement: batched right-preconditioned GMRES (fast.py:658-663, 1437-1500) -----------------------------
+    def refine(self, A, B, M, restart, stall=None, predict=True):
+        """fast.py:658-663: GMRES to MIXED_RTOL, one cycle of at most `restart` iterations; (Y, converged, largest
+        relative residual of B - A Y)."""
+        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, stall=stall, predict=predict)
         R = B - A(Y)
         rn = np.sqrt(np.abs(self._dotc(R, R)))
         bn = np.sqrt(np.abs(self._dotc(B, B)))
@@ -445,89 +435,68 @@ class DirectSolver:
         self.residual = rel
         return Y, bool(np.isfinite(rel).all() and (rel <= 100 * MIXED_RTOL).all()), float(rel.max())
 
-    def gmres_batched(self, A, B, M=None, rtol=1e-6, restart=30, maxiter=10, stall=None, predict=True):
-        """fast.py:1437-1500 on device vectors: right-preconditioned restarted GMRES for k systems in lockstep,
-        modified Gram-Schmidt, conjugated Givens rotations, the stall rule. The (restart x restart) Hessenberg
-        recurrences run on the host."""
+    def gmres_batched(self, A, B, M, rtol=1e-6, restart=30, stall=None, predict=True):
+        """Right-preconditioned GMRES on A Y = B for the k columns of B at once, one cycle from Y = 0, the role of
+        the reference's gmres_batched (fast.py:1437-1500) as its callers use it (maxiter 1, fast.py:1053):
+
+        - the Krylov bases of all columns advance together: the directions Z_j = M(V_j) and A Z_j are N x k
+          blocks, and m25_arnoldi_orth orthogonalises A Z_j against V_0 .. V_j (classical Gram-Schmidt applied
+          twice) and normalises it into V_{j+1} on the device, leaving the Hessenberg column there;
+        - the host reads that column (the one synchronisation of a step) and, for each column still iterating,
+          solves the small least-squares problem min |beta e_1 - H y| by a complete QR of H, whose last
+          transformed entry is the residual norm;
+        - a column whose residual reaches rtol |b| stops there (its y from that step); the others go on;
+        - stall = (n, x): after n steps, a column still above x |b| ends the iteration for all (the reference's
+          FRESH_STALL rule, fast.py:256); with predict, after PREDICT_AFTER steps a column whose geometric rate
+          so far would leave it 10x above the tolerance at the last step also ends it (the caller will solve in
+          double precision: the steps that remain would be lost);
+        - Y = sum_j Z_j y_j, one device product per step used.
+        Returns (Y, iterations per column)."""
         N, k = B.shape
-        X = torch.zeros_like(B)
-        M = M or (lambda R: R.clone())
         bn = np.sqrt(np.abs(self._dotc(B, B)))
         bn[bn == 0] = 1.0
-        iters, act = np.zeros(k, int), np.arange(k)
-        started = False
-        for _ in range(maxiter):
-            Xa = X[:, act].contiguous()
-            R = B[:, act].contiguous()
-            if started:
-                R = R - A(Xa)
-            beta = np.sqrt(np.abs(self._dotc(R, R)))
-            done = beta <= rtol * bn[act]
-            keep = np.flatnonzero(~done)
-            act, beta = act[keep], beta[keep]
-            if not len(act):
+        V = self._buf('krylov', (restart + 1, N, k), torch.complex128)
+        Zd = self._buf('krylov_z', (restart, N, k), torch.complex128)
+        hcol = self._buf('hcol', (restart + 1, k), torch.complex128)
+        htmp = self._buf('htmp', (restart + 1, k), torch.complex128)
+        # V_0 = B / |B| per column
+        self._scale(B, s_cols=1.0 / bn, out=V[0])
+        H = np.zeros((k, restart + 1, restart), complex)
+        rhs = np.zeros((k, restart + 1), complex)
+        rhs[:, 0] = bn
+        steps = np.zeros(k, int)              # steps each column takes (its y has that many entries)
+        done = np.zeros(k, bool)
+        res = bn.copy()
+        for j in range(restart):
+            Zd[j].copy_(M(V[j]))
+            W = A(Zd[j]).contiguous()
+            check(lib().m25_arnoldi_orth(P(V), c_int(j), c_long(N), c_int(k), P(W), P(hcol), P(htmp), self.s),
+                  'm25_arnoldi_orth')
+            H[:, :j + 2, j] = hcol[:j + 2].cpu().numpy().T
+            live = np.flatnonzero(~done)
+            Q, _ = np.linalg.qr(H[live, :j + 2, :j + 1], mode='complete')
+            g = np.einsum('cji,cj->ci', Q.conj(), rhs[live, :j + 2])
+            res[live] = np.abs(g[:, j + 1])
+            steps[live] = j + 1
+            done[live] |= res[live] <= rtol * bn[live]
+            if done.all():
                 break
-            R = R[:, torch.as_tensor(keep, device='cuda')].contiguous()
-            ka = len(act)
-            Vall = torch.empty((restart + 1, N, ka), dtype=torch.complex128, device='cuda')   # the Krylov basis
-            V, Zk = [Vall[i] for i in range(restart + 1)], [None] * restart
-            H = np.zeros((restart + 1, restart, ka), complex)
-            g = np.zeros((restart + 1, ka), complex)
-            cs, sn = np.zeros((restart, ka), complex), np.zeros((restart, ka), complex)
-            g[0] = beta
-            self._scale(R, s_cols=1.0 / beta, out=V[0])
-            live, last, stalled = np.ones(ka, bool), np.full(ka, restart - 1), False
-            for j in range(restart):
-                Zk[j] = M(V[j])
-                Wv = A(Zk[j]).contiguous()
-                # orthogonalised against V[0 .. j] by classical Gram-Schmidt applied twice: two batched products
-                # a pass instead of one a basis vector (the reference's modified Gram-Schmidt, fast.py:1473-1476, to
-                # the same rounding level)
-                hj = np.zeros((j + 1, ka), complex)
-                for _ in range(2):
-                    h = self._dotc_multi(Vall, j + 1, Wv)
-                    self._axpy_multi(Wv, Vall, j + 1, h)
-                    hj += h
-                H[:j + 1, j] = hj
-                hn = np.sqrt(np.abs(self._dotc(Wv, Wv)))
-                H[j + 1, j] = hn
-                self._scale(Wv, s_cols=1.0 / np.where(hn > 0, hn, 1), out=V[j + 1])
-                for i in range(j):
-                    H[i, j], H[i + 1, j] = (cs[i] * H[i, j] + sn[i] * H[i + 1, j],
-                                            -np.conj(sn[i]) * H[i, j] + np.conj(cs[i]) * H[i + 1, j])
-                den = np.sqrt(np.abs(H[j, j]) ** 2 + np.abs(H[j + 1, j]) ** 2)
-                den[den == 0] = 1.0
-                cs[j], sn[j] = H[j, j].conj() / den, H[j + 1, j].conj() / den
-                H[j, j], H[j + 1, j] = cs[j] * H[j, j] + sn[j] * H[j + 1, j], 0
-                g[j + 1], g[j] = -np.conj(sn[j]) * g[j], cs[j] * g[j]
-                iters[act[live]] += 1
-                conv = live & (np.abs(g[j + 1]) <= rtol * bn[act])
-                last[conv] = j
-                live &= ~conv
-                if not live.any():
-                    break
-                if stall is not None and j + 1 >= stall[0] and (np.abs(g[j + 1])[live] > stall[1] * bn[act][live]).any():
-                    last[live], stalled = j, True
-                    break
-                if stall is not None and predict and j + 1 >= PREDICT_AFTER:
-                    # the residual's geometric rate so far, extrapolated to the last iteration: a column that would
-                    # still be 10x above the tolerance there ends the refinement now (its iterations would be lost:
-                    # the caller solves in double precision either way)
-                    r0, rj = np.abs(g[0])[live], np.abs(g[j + 1])[live]
-                    rate = (rj / np.maximum(r0, 1e-300)) ** (1.0 / (j + 1))
-                    if (rj * rate ** (restart - j - 1) > 10 * rtol * bn[act][live]).any():
-                        last[live], stalled = j, True
-                        break
-            ys = []
-            for c in range(ka):
-                m = last[c] + 1
-                ys.append(np.linalg.solve(np.triu(H[:m, :m, c]), g[:m, c]) if m else np.zeros(0))
-            Xa = X[:, act].contiguous()
-            for j in range(max(last) + 1):
-                a = np.array([ys[c][j] if j < len(ys[c]) else 0.0 for c in range(ka)], complex)
-                self._axpy(Xa, Zk[j], a)
-            X[:, torch.as_tensor(act, device='cuda')] = Xa
-            started = True
-            if stalled:
+            act = ~done
+            if stall is not None and j + 1 >= stall[0] and (res[act] > stall[1] * bn[act]).any():
                 break
-        return X, iters.tolist()
+            if stall is not None and predict and j + 1 >= PREDICT_AFTER:
+                rate = (res[act] / bn[act]) ** (1.0 / (j + 1))
+                if (res[act] * rate ** (restart - j - 1) > 10 * rtol * bn[act]).any():
+                    break
+        # y per column from its own steps, Y = sum_j Z_j y_j
+        m = int(steps.max())
+        coef = np.zeros((m, k), complex)
+        for c in range(k):
+            s_c = steps[c]
+            Q, R = np.linalg.qr(H[c, :s_c + 1, :s_c], mode='complete')
+            g = Q.conj().T @ rhs[c, :s_c + 1]
+            coef[:s_c, c] = np.linalg.solve(np.triu(R[:s_c, :s_c]), g[:s_c])
+        Y = torch.zeros((N, k), dtype=torch.complex128, device='cuda')
+        if m:
+            self._axpy_multi(Y, Zd, m, -coef)
+        return Y, steps.tolist()

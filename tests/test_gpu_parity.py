@@ -311,3 +311,25 @@ def test_complex64_solves_over_several_blocks_a_cta(n, nrhs):
         _lib.sync_check()
         err = (X.to(torch.complex128) - x).abs().max().item() / x.abs().max().item()
         assert err < 1e-4, err
+
+
+@pytest.mark.parametrize('k', [1, 3, 8])
+def test_gmres_batched_matches_a_direct_solve(small, k):
+    """The refinement's GMRES (device Arnoldi steps, host least squares) on a dense system with a nearby
+    preconditioner: every column converges to the direct solution; columns stop on their own at the tolerance."""
+    geo, ds, od = small
+    n = 400
+    rng = np.random.default_rng(3 + k)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 2 * np.sqrt(n) * np.eye(n)
+    Pinv = np.linalg.inv(A + 3e-4 * np.abs(A).max() * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))))
+    B = rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))
+    B[:, 0] *= 1e3                                         # columns of very different sizes
+    Ad, Pd, Bd = (torch.from_numpy(x).to('cuda') for x in (A, Pinv, B))
+    Y, it = ds.gmres_batched(lambda V: Ad @ V, Bd, lambda R: Pd @ R, rtol=1e-12, restart=30)
+    X = np.linalg.solve(A, B)
+    Yh = Y.cpu().numpy()
+    assert (np.abs(Yh - X).max(0) <= 1e-9 * np.abs(X).max(0)).all(), it
+    assert max(it) <= 20 and min(it) >= 1
+    # a preconditioner that does not help within the stall rule's window ends the iteration early
+    Y2, it2 = ds.gmres_batched(lambda V: Ad @ V, Bd, lambda R: 0 * R + R, rtol=1e-12, restart=30, stall=(4, 1e-9))
+    assert max(it2) == 4

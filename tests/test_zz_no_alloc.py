@@ -51,3 +51,61 @@ def test_noalloc_solves_match_getrs_twice(single):
         assert np.abs(b - a).max() <= tol * np.abs(a).max(), call
         x = np.linalg.solve(Z.astype(complex), R.astype(complex))
         assert np.abs(b - x).max() <= (1e-4 if single else 1e-11) * np.abs(x).max(), call
+
+
+def _pool_high_water(rt, pool):
+    err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemHigh)
+    assert int(err) == 0
+    return int(v)
+
+
+@pytest.mark.gpu
+def test_noalloc_solve_takes_no_device_memory():
+    """The property the entry point exists for: the stream-ordered pool's high-water mark (reset before each call)
+    moves for the allocating solve, m25_getrs, and stays where it was for m25_getrs_noalloc; torch's caching
+    allocator sees no allocation during the no-alloc call either."""
+    from cuda.bindings import driver as cu, runtime as rt
+    from mom25d_b200 import _lib
+    L = _lib.lib()
+    n, k, single = 1200, 2, 1
+    rng = np.random.default_rng(12)
+    Z = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)) + 4 * np.sqrt(n) * np.eye(n)).astype(np.complex64)
+    Zd = _lib.dev(Z)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(L.m25_getrf_workspace(n, single))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    s = _lib.stream_ptr()
+    _lib.check(L.m25_getrf(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, 0, _lib.P(work),
+                           ctypes.c_size_t(nb), s), 'm25_getrf')
+    R = _lib.dev((rng.standard_normal((n, k)) + 1j * rng.standard_normal((n, k))).astype(np.complex64))
+    Rb = R.clone()
+    # first call on this device: the no-alloc entry point's once-per-device set-up happens here
+    _lib.check(L.m25_getrs_noalloc(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, _lib.P(Rb), k, s),
+               'm25_getrs_noalloc')
+    _lib.sync_check(what='first no-alloc solve')
+    dev = torch.cuda.current_device()
+    err, pool = rt.cudaDeviceGetMemPool(dev)
+    assert int(err) == 0
+    def reset():
+        r = rt.cudaMemPoolSetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemHigh, cu.cuuint64_t(0))
+        assert int(r[0] if isinstance(r, tuple) else r) == 0
+    torch.cuda.synchronize()
+    reset()
+    base = _pool_high_water(rt, pool)
+    Ra = R.clone()
+    _lib.check(L.m25_getrs(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, _lib.P(Ra), k, s), 'm25_getrs')
+    _lib.sync_check(what='allocating solve')
+    assert _pool_high_water(rt, pool) > base             # the check sees an allocation when there is one
+    torch.cuda.synchronize()
+    reset()
+    base = _pool_high_water(rt, pool)
+    Rb = R.clone()
+    torch.cuda.synchronize()
+    allocs = torch.cuda.memory_stats().get('allocation.all.allocated', 0)
+    _lib.check(L.m25_getrs_noalloc(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, _lib.P(Rb), k, s),
+               'm25_getrs_noalloc')
+    _lib.sync_check(what='no-alloc solve')
+    assert _pool_high_water(rt, pool) == base
+    assert torch.cuda.memory_stats().get('allocation.all.allocated', 0) == allocs
+    a, b = Ra.cpu().numpy(), Rb.cpu().numpy()
+    assert np.abs(b - a).max() <= 1e-5 * np.abs(a).max()
