@@ -69,36 +69,39 @@ class LayerStack:
         return max([abs(l.er_c) for l in self.layers] + ([abs(self.top_er)] if self.top == 'open' else []))
 
     def nearest_discontinuity(self, k):
-        """multilayer.py:172-178: distance from interface k to the closest permittivity step or ground."""
-        down = next((self.z[k] - self.z[j] for j in range(k - 1, -1, -1)
-                     if self.is_pec(j) or self.eps(j) != self.eps(j + 1)), np.inf)
-        up = next((self.z[j] - self.z[k] for j in range(k + 1, self.N + 1)
-                   if self.is_pec(j) or self.eps(j) != self.eps(j + 1)), np.inf)
-        return min(down, up)
+        """How far interface k is from the nearest interface, below or above it, where the permittivity steps or
+        a PEC lies (the image term's reach, multilayer.py:170-176); inf where there is none."""
+        def steps(j):
+            return self.is_pec(j) or self.eps(j) != self.eps(j + 1)
+        gaps = [abs(self.z[k] - self.z[j]) for j in range(self.N + 1) if j != k and steps(j)]
+        return min(gaps, default=np.inf)
 
 
 # ---- mesher -------------------------------------------------------------------------------------------------------
 def graded(u, grade):
-    """base.py:80-82: u in 0..1 graded toward both ends (cosine)."""
+    """Positions u in [0, 1] pulled toward both ends by a cosine (grade 0: uniform, 1: fully cosine), the
+    reference's cell grading across a strip (base.py:80-82)."""
     return (1 - grade) * u + grade * (1 - np.cos(np.pi * u)) / 2
 
 
 def _axis_lines(edge_vals, port_vals, dmax, ncross, narrow, grade=0.0):
-    """multilayer.py:322-335: grid lines along one axis: ncross graded cells across narrow intervals, cells of at
-    most dmax elsewhere, port / via lines kept."""
-    e = np.unique(np.round(np.asarray(edge_vals, float), 12))
-    pv = np.unique(np.round(np.asarray(port_vals, float), 12))
-    out = [e[0]]
-    for a, b in zip(e[:-1], e[1:]):
-        inner = [p for p in pv if a + 1e-9 < p < b - 1e-9]
-        if b - a <= narrow + 1e-12 and not inner:
-            out.extend(a + (b - a) * graded(np.linspace(0, 1, ncross + 1)[1:], grade))
+    """Grid coordinates along one axis, the same numbers as the reference's axis lines (multilayer.py:321-335):
+    the distinct conductor-edge coordinates; between two neighbours at most `narrow` apart with no line to keep
+    strictly inside them (a strip across its width), ncross cells graded toward both ends; every other interval
+    is split at the lines to keep (ports, vias, cut lines) and each piece cut evenly into cells of at most dmax."""
+    edges = np.unique(np.round(np.asarray(edge_vals, float), 12))
+    pins = np.unique(np.round(np.asarray(port_vals, float), 12))
+    pieces = [edges[:1]]
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        inside = pins[(pins > lo + 1e-9) & (pins < hi - 1e-9)]
+        if inside.size == 0 and hi - lo <= narrow + 1e-12:
+            pieces.append(lo + (hi - lo) * graded(np.linspace(0, 1, ncross + 1)[1:], grade))
             continue
-        bps = [a] + inner + [b]
-        for c, d in zip(bps[:-1], bps[1:]):
-            n = max(1, int(np.ceil((d - c) / dmax - 1e-9)))
-            out.extend(np.linspace(c, d, n + 1)[1:])
-    return np.array(out)
+        stops = np.concatenate([[lo], inside, [hi]])
+        for c, d in zip(stops[:-1], stops[1:]):
+            cells = max(1, int(np.ceil((d - c) / dmax - 1e-9)))
+            pieces.append(np.linspace(c, d, cells + 1)[1:])
+    return np.concatenate(pieces)
 
 
 def tensor_mesh(rects, dmax, ncross, narrow, xlines=(), ylines=(), grade=1.0):
@@ -216,6 +219,65 @@ class GapPort:
         self.layer, self.c, self.d = int(layer), np.asarray(center, float), d / np.linalg.norm(d)
         self.t = np.array([-self.d[1], self.d[0]])
         self.w, self.zc, self.name = float(width), float(z0), name
+
+
+class LinePort:
+    """A wave port on a straight feed (the reference's geo.LinePort, geo.py:24-56): a delta-gap source across the
+    feed at `center`, `direction` pointing into the device along the feed, `width` the feed's width (the gap and
+    the sample cuts span it); the reference plane `ref_dist` from the gap along the feed; sample cuts from s0 to s1
+    every `step` (defaults 2 step, ref_dist and dmax), on which the forward and backward waves of the feed are fitted.
+    zc: the reference impedance (zc_fn(f), where set, replaces it at each frequency); gamma_fn(f): a known
+    propagation constant of the feed (from a line characterisation) used instead of fitting one."""
+    kind = 'wave'
+
+    def __init__(self, layer, center, direction, width, ref_dist, s0=None, step=None, zc=50.0, name='', s1=None):
+        d = np.asarray(direction, float)
+        self.layer, self.c, self.d = int(layer), np.asarray(center, float), d / np.linalg.norm(d)
+        self.t = np.array([-self.d[1], self.d[0]])
+        self.w, self.ref, self.s0, self.step, self.s1 = float(width), float(ref_dist), s0, step, s1
+        self.zc, self.name = float(zc), name
+        self.zc_fn = self.gamma_fn = None
+
+    def line(self, s):
+        """The ends of the transverse line at distance s from the gap along the feed."""
+        p = self.c + self.d * s
+        return p - self.t * self.w / 2, p + self.t * self.w / 2
+
+    @property
+    def axis_aligned(self):
+        return abs(self.d[0]) < 1e-12 or abs(self.d[1]) < 1e-12
+
+    def sample_positions(self, dmax):
+        """The sample cuts' distances from the gap (sim.py:426-431): s1, s1 - step, ... down to no closer than s0,
+        in increasing order."""
+        step = self.step or dmax
+        s0 = 2 * step if self.s0 is None else self.s0
+        s1 = self.ref if self.s1 is None else self.s1
+        count = int(np.floor((s1 - s0) / step + 1e-9)) + 1
+        return s1 - step * np.arange(count)[::-1]
+
+
+def port_lines(ports, lumped, dmax):
+    """{interface: (x lines, y lines)}: the mesh lines the ports and lumped elements need (sim.py:424-440): a gap
+    port's and a lumped element's cut, a wave port's gap and every sample cut. Axis-aligned feeds only (the
+    tensor mesher)."""
+    lines = {}
+
+    def add(lp, at):
+        if not (abs(lp.d[0]) < 1e-12 or abs(lp.d[1]) < 1e-12):
+            raise ValueError("ports and lumped elements on the tensor mesh run along x or y")
+        xs, ys = lines.setdefault(lp.layer, ([], []))
+        along_x = abs(lp.d[0]) > 0.5
+        for s in at:
+            (xs if along_x else ys).append(float((lp.c + lp.d * s)[0 if along_x else 1]))
+    for p in ports:
+        if isinstance(p, LinePort):
+            add(p, np.append(p.sample_positions(dmax), 0.0))
+        elif isinstance(p, GapPort):
+            add(p, [0.0])
+    for el in lumped:
+        add(el.lp, [0.0])
+    return lines
 
 
 @dataclass

@@ -187,154 +187,179 @@ __global__ void k_far_block(const int *R_, int nr, const int *C_, int nc, double
     stc<double>(out, idx, v);
 }
 
-// ---- analytic 1/sqrt(rho^2 + d^2) moments (mom25d_core.cpp:321-365) ---------------------------------------------------
-__device__ __forceinline__ bool rule_over_p(double ap, double aq, int p, int q)
+// ---- near-field correction (the reference's near_core, mom25d_core.cpp:417-507): a half warp per near pair ---------
+// A near pair (p, q) of triangles gets: the smooth rest of the tabulated kernel integrated by the 3-point (same
+// interface) or 6-point (across interfaces) rule on both triangles; plus each extracted singular part c / sqrt(rho^2
+// + d^2) integrated analytically over one triangle of the pair with the 6-point rule over the other (the rule goes
+// on the smaller triangle, ties by index: mom25d_core.cpp:321-324); minus the centroid value the far fill put there.
+// What is integrated are seven moments: 1, r, r', r.r' against G_A and 1 against G_q (r on p, r' on q); the 3 x 3
+// values of the edge pairs (halves on p) x (halves on q) are combinations of them.
+//
+// On the GPU, 16 lanes (a half warp) carry one pair, two pairs a warp:
+//  1. the np^2 quadrature point pairs (9 or 36) are dealt out over the 16 lanes, each lane sums its share of the
+//     seven moments, and a butterfly of shuffles inside the half warp gives every lane the totals;
+//  2. the analytic moments (computed at the first frequency only: `stat` keeps them, they do not depend on it) deal
+//     out their 18 (rule point, triangle side) line integrals the same way;
+//  3. lanes 0 .. 8 each form one of the 3 x 3 edge-pair values and add it into Z (mode 0) or write it as a COO
+//     triplet (mode 2, slot 9 i + 3 s + u, row -1 where a half is missing).
+// The line integrals of 1/R and of the in-plane offset over a triangle side seen from a point at height d are the
+// closed forms of Wilton et al. (IEEE Trans. AP 32, 1984) and Graglia (IEEE Trans. AP 41, 1993).
+
+__device__ __forceinline__ bool rule_on_p(double ap, double aq, int p, int q)
 {
     const double tie = 1e-9 * fmax(ap, aq);
     return fabs(ap - aq) <= tie ? p <= q : ap < aq;
 }
 
-__device__ void offplane_one(const double *V, const double *P6, const double *W6, double d, double m[6], bool keep)
+__device__ __forceinline__ double half_sum(double v, unsigned mask)
 {
-    double ad = fabs(d);
-    double e[3][2], L[3], tau[3][2], un[3][2];
-    for (int i = 0; i < 3; ++i) {
-        int j = (i + 1) % 3;
-        e[i][0] = V[2 * j] - V[2 * i]; e[i][1] = V[2 * j + 1] - V[2 * i + 1];
-        L[i] = sqrt(e[i][0] * e[i][0] + e[i][1] * e[i][1]);
-        tau[i][0] = e[i][0] / L[i]; tau[i][1] = e[i][1] / L[i];
-        un[i][0] = tau[i][1]; un[i][1] = -tau[i][0];
-    }
-    double m0 = 0, mro0 = 0, mro1 = 0, mrs0 = 0, mrs1 = 0, mrr = 0;
-    for (int k = 0; k < 6; ++k) {
-        double rx = P6[2 * k], ry = P6[2 * k + 1], wq = W6[k];
-        double I1 = 0, IRx = 0, IRy = 0;
-        for (int i = 0; i < 3; ++i) {
-            double dvx = V[2 * i] - rx, dvy = V[2 * i + 1] - ry;
-            double sm = dvx * tau[i][0] + dvy * tau[i][1];
-            double sp = sm + L[i];
-            double t0 = dvx * un[i][0] + dvy * un[i][1];
-            double R02 = t0 * t0 + d * d, R0 = sqrt(R02);
-            double Rm = sqrt(R02 + sm * sm), Rp = sqrt(R02 + sp * sp);
-            double lg = (R0 > 1e-14 * L[i]) ? asinh(sp / R0) - asinh(sm / R0) : 0.0;
-            double beta = atan2(t0 * sp, R02 + ad * Rp) - atan2(t0 * sm, R02 + ad * Rm);
-            I1 += t0 * lg - ad * beta;
-            double eR = 0.5 * (R02 * lg + sp * Rp - sm * Rm);
-            IRx += eR * un[i][0]; IRy += eR * un[i][1];
-        }
-        double Wx = IRx + rx * I1, Wy = IRy + ry * I1;
-        m0 += wq * I1;
-        mro0 += wq * rx * I1; mro1 += wq * ry * I1;
-        mrs0 += wq * Wx; mrs1 += wq * Wy;
-        mrr += wq * (rx * Wx + ry * Wy);
-    }
-    // observation- / source-weighted moments handed back as (p, q) whichever triangle carried the rule
-    m[0] = m0;
-    if (keep) { m[1] = mro0; m[2] = mro1; m[3] = mrs0; m[4] = mrs1; }
-    else { m[1] = mrs0; m[2] = mrs1; m[3] = mro0; m[4] = mro1; }
-    m[5] = mrr;
+    v += __shfl_xor_sync(mask, v, 8, 16);
+    v += __shfl_xor_sync(mask, v, 4, 16);
+    v += __shfl_xor_sync(mask, v, 2, 16);
+    v += __shfl_xor_sync(mask, v, 1, 16);
+    return v;
 }
 
-// ---- near-field correction (near_core, mom25d_core.cpp:417-507) -----------------------------------------------------
-// One thread per near pair. mode 0: atomically added into Z (R_out = double or float); mode 2: COO triplets.
+__device__ __forceinline__ zd half_sum(zd v, unsigned mask) { return mk<double>(half_sum(v.x, mask), half_sum(v.y, mask)); }
+
+// The line integral of side `side` of triangle `tri` (counter-clockwise) seen from the point r at height d:
+// this side's part of I1 = int 1/R dS' and of IR = int (r' - r)/R dS' (in-plane) over the triangle.
+__device__ __forceinline__ void side_integrals(const m25_quad &q, int tri, int side, double rx, double ry, double d,
+                                               double &I1, double &IRx, double &IRy)
+{
+    const int n0 = q.tris[3 * tri + side], n1 = q.tris[3 * tri + (side == 2 ? 0 : side + 1)];
+    const double v0x = q.nodes[2 * n0], v0y = q.nodes[2 * n0 + 1];
+    const double ex = q.nodes[2 * n1] - v0x, ey = q.nodes[2 * n1 + 1] - v0y;
+    const double len = sqrt(ex * ex + ey * ey);
+    const double tx = ex / len, ty = ey / len;             // along the side; (ty, -tx) points out of the triangle
+    const double ox = v0x - rx, oy = v0y - ry;
+    const double s0 = ox * tx + oy * ty, s1 = s0 + len;    // the side's ends along it, from the foot of r
+    const double h = ox * ty - oy * tx;                    // signed in-plane distance of r from the side's line
+    const double ad = fabs(d);
+    const double rho2 = h * h + d * d, rho = sqrt(rho2);
+    const double R0 = sqrt(rho2 + s0 * s0), R1 = sqrt(rho2 + s1 * s1);
+    const double lg = rho > 1e-14 * len ? asinh(s1 / rho) - asinh(s0 / rho) : 0.0;
+    const double ang = atan2(h * s1, rho2 + ad * R1) - atan2(h * s0, rho2 + ad * R0);
+    I1 = h * lg - ad * ang;
+    const double e = 0.5 * (rho2 * lg + s1 * R1 - s0 * R0);
+    IRx = e * ty;
+    IRy = -e * tx;
+}
+
 template <typename Zt>
-__device__ __forceinline__ void atomic_add_c(Zt *Z, size_t i, zd v);
-template <> __device__ __forceinline__ void atomic_add_c<double>(double *Z, size_t i, zd v)
+__device__ __forceinline__ void add_to_z(Zt *Z, size_t i, zd v);
+template <> __device__ __forceinline__ void add_to_z<double>(double *Z, size_t i, zd v)
 {
     atomicAdd(Z + 2 * i, v.x); atomicAdd(Z + 2 * i + 1, v.y);
 }
-template <> __device__ __forceinline__ void atomic_add_c<float>(float *Z, size_t i, zd v)
+template <> __device__ __forceinline__ void add_to_z<float>(float *Z, size_t i, zd v)
 {
     atomicAdd(Z + 2 * i, (float)v.x); atomicAdd(Z + 2 * i + 1, (float)v.y);
 }
 
 template <typename Zt>
-__global__ void __launch_bounds__(128) k_near(int mode, Zt *Z, long ld, int *ri, int *ci, double *vv, double *qcorr,
+__global__ void __launch_bounds__(256) k_near(int mode, Zt *Z, long ld, int *ri, int *ci, double *vv, double *qcorr,
                                               double *stat, int stat_ready, m25_mesh g, m25_tables tb, m25_quad q,
                                               const int *P, const int *Q, long n, double w, int *err)
 {
-    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const zd jw = mk<double>(0, w), inv_jw = mk<double>(0, -1.0 / w);
+    const long i = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 4;     // the pair of this half warp
+    if (i >= n) return;                                                   // (whole half warps leave together)
+    const int l = threadIdx.x & 15;
+    const unsigned mask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
     const int p = P[i], qq = Q[i];
-    if (p < 0 || p >= g.Nt || qq < 0 || qq >= g.Nt) { dev_error(err, M25_DEV_INDEX); return; }
+    if (p < 0 || p >= g.Nt || qq < 0 || qq >= g.Nt) {
+        if (l == 0) dev_error(err, M25_DEV_INDEX);
+        return;
+    }
     const int la = g.lt[p], lb = g.lt[qq];
     const int t = tb.tab[la * tb.L + lb];
-    const bool same = (la == lb);
-    const int np = same ? 3 : 6;
-    const double *Pa = same ? q.P3 + 6 * (size_t)p : q.P6 + 12 * (size_t)p;
-    const double *Pb = same ? q.P3 + 6 * (size_t)qq : q.P6 + 12 * (size_t)qq;
-    const double *Wa = same ? q.W3 + 3 * (size_t)p : q.W6 + 6 * (size_t)p;
-    const double *Wb = same ? q.W3 + 3 * (size_t)qq : q.W6 + 6 * (size_t)qq;
-    zd M0 = mk<double>(0, 0), Mox = M0, Moy = M0, Msx = M0, Msy = M0, Mrr = M0, Mq = M0;
-    double pbx[6], pby[6], wb[6];
-    for (int b = 0; b < np; ++b) { pbx[b] = Pb[2 * b]; pby[b] = Pb[2 * b + 1]; wb[b] = Wb[b]; }
-    for (int a = 0; a < np; ++a) {
-        const double pax = Pa[2 * a], pay = Pa[2 * a + 1], wa = Wa[a];
-        for (int b = 0; b < np; ++b) {
-            double dx = pax - pbx[b], dy = pay - pby[b];
-            zd ga, gq;
-            tab_rest<double>(tb, t, sqrt(dx * dx + dy * dy), ga, gq);
-            double wt = wa * wb[b];
-            ga = ga * wt; gq = gq * wt;
-            M0 += ga; Mox += ga * pax; Moy += ga * pay;
-            Msx += ga * pbx[b]; Msy += ga * pby[b];
-            Mrr += ga * (pax * pbx[b] + pay * pby[b]);
-            Mq += gq;
-        }
-    }
-    const bool keep = rule_over_p(g.area[p], g.area[qq], p, qq);
-    const int po = keep ? p : qq, qi = keep ? qq : p;
-    double V[6];
-    for (int k = 0; k < 3; ++k) {
-        int nd = q.tris[3 * qi + k];
-        V[2 * k] = q.nodes[2 * nd]; V[2 * k + 1] = q.nodes[2 * nd + 1];
-    }
-    const int kd = tb.kind[t];
-    const int nk = kd == 0 ? (tb.dimg[t] > 0 ? 2 : 1) : (kd == 1 ? 1 : 0);
-    for (int k = 0; k < nk; ++k) {
-        double dd = kd == 0 ? (k == 0 ? 0.0 : tb.dimg[t]) : tb.d[t];
-        zd cA = (k == 0) ? ldc<double>(tb.cA, t) : ldc<double>(tb.cAi, t);
-        zd cq = (k == 0) ? ldc<double>(tb.cq, t) : ldc<double>(tb.cqi, t);
-        double m[6];
-        double *st = stat ? stat + 12 * (size_t)i + 6 * k : nullptr;
-        if (st && stat_ready) {
-            for (int j = 0; j < 6; ++j) m[j] = st[j];
-        } else {
-            offplane_one(V, q.P6 + 12 * (size_t)po, q.W6 + 6 * (size_t)po, dd, m, keep);
-            if (st) for (int j = 0; j < 6; ++j) st[j] = m[j];
-        }
-        M0 += cA * m[0]; Mox += cA * m[1]; Moy += cA * m[2]; Msx += cA * m[3]; Msy += cA * m[4];
-        Mrr += cA * m[5]; Mq += cq * m[0];
-    }
-    {
-        double r = cdist<double>(g.cent, p, qq);
+    const int np = la == lb ? 3 : 6;
+    const double *Pa = np == 3 ? q.P3 + 6 * (size_t)p : q.P6 + 12 * (size_t)p;
+    const double *Pb = np == 3 ? q.P3 + 6 * (size_t)qq : q.P6 + 12 * (size_t)qq;
+    const double *Wa = np == 3 ? q.W3 + 3 * (size_t)p : q.W6 + 6 * (size_t)p;
+    const double *Wb = np == 3 ? q.W3 + 3 * (size_t)qq : q.W6 + 6 * (size_t)qq;
+    // 1. the smooth rest by quadrature: moments 1, r (obs), r' (src), r.r' of G_A and 1 of G_q
+    zd s1 = mk<double>(0, 0), sox = s1, soy = s1, ssx = s1, ssy = s1, srr = s1, sq = s1;
+    for (int k = l; k < np * np; k += 16) {
+        const int a = k / np, b = k - a * np;
+        const double ax = Pa[2 * a], ay = Pa[2 * a + 1], bx = Pb[2 * b], by = Pb[2 * b + 1];
+        const double dx = ax - bx, dy = ay - by;
         zd ga, gq;
-        tab_kern<double>(tb, la, lb, r, ga, gq);
-        double wgt = g.area[p] * g.area[qq];
-        double cpx_ = g.cent[2 * p], cpy = g.cent[2 * p + 1], cqx = g.cent[2 * qq], cqy = g.cent[2 * qq + 1];
-        ga = ga * wgt; gq = gq * wgt;
-        M0 -= ga; Mox -= ga * cpx_; Moy -= ga * cpy; Msx -= ga * cqx; Msy -= ga * cqy;
-        Mrr -= ga * (cpx_ * cqx + cpy * cqy); Mq -= gq;
+        tab_rest<double>(tb, t, sqrt(dx * dx + dy * dy), ga, gq);
+        const double wt = Wa[a] * Wb[b];
+        ga = ga * wt;
+        s1 += ga; sox += ga * ax; soy += ga * ay; ssx += ga * bx; ssy += ga * by;
+        srr += ga * (ax * bx + ay * by);
+        sq += gq * wt;
     }
-    if (qcorr) stc<double>(qcorr, i, Mq);
-    for (int s = 0; s < 3; ++s) {
-        int em_ = g.te[3 * p + s];
-        for (int u = 0; u < 3; ++u) {
-            int en = g.te[3 * qq + u];
-            size_t slot = 9 * (size_t)i + 3 * s + u;
-            if (em_ < 0 || en < 0) {
-                if (mode == 2) { ri[slot] = -1; ci[slot] = 0; vv[2 * slot] = 0; vv[2 * slot + 1] = 0; }
-                continue;
+    s1 = half_sum(s1, mask); sox = half_sum(sox, mask); soy = half_sum(soy, mask);
+    ssx = half_sum(ssx, mask); ssy = half_sum(ssy, mask); srr = half_sum(srr, mask); sq = half_sum(sq, mask);
+    // 2. the extracted singular parts: the rule on the smaller triangle, the closed form over the other
+    const bool obs_rule = rule_on_p(g.area[p], g.area[qq], p, qq);
+    const int tr = obs_rule ? p : qq, ta = obs_rule ? qq : p;
+    const int kd = tb.kind[t];
+    const int nsing = kd == 0 ? (tb.dimg[t] > 0 ? 2 : 1) : (kd == 1 ? 1 : 0);
+    for (int x = 0; x < nsing; ++x) {
+        const double d = kd == 0 ? (x == 0 ? 0.0 : tb.dimg[t]) : tb.d[t];
+        double m[6];                                       // 1, r (obs) x/y, r' (src) x/y, r.r'
+        double *kept = stat ? stat + 12 * (size_t)i + 6 * x : nullptr;
+        if (kept && stat_ready) {
+            for (int c = 0; c < 6; ++c) m[c] = kept[c];
+        } else {
+            double c0 = 0, crx = 0, cry = 0, cax = 0, cay = 0, crr = 0;    // rule-side r, analytic-side r'
+            for (int e = l; e < 18; e += 16) {
+                const int kq = e / 3, side = e - 3 * kq;
+                const double rx = q.P6[12 * (size_t)tr + 2 * kq], ry = q.P6[12 * (size_t)tr + 2 * kq + 1];
+                const double wq = q.W6[6 * (size_t)tr + kq];
+                double I1, IRx, IRy;
+                side_integrals(q, ta, side, rx, ry, d, I1, IRx, IRy);
+                const double Ax = IRx + rx * I1, Ay = IRy + ry * I1;       // int r'/R
+                c0 += wq * I1;
+                crx += wq * rx * I1; cry += wq * ry * I1;
+                cax += wq * Ax; cay += wq * Ay;
+                crr += wq * (rx * Ax + ry * Ay);
             }
-            double am_ = g.ta[3 * p + s], vx = g.tv[6 * p + 2 * s], vy = g.tv[6 * p + 2 * s + 1];
-            double an = g.ta[3 * qq + u], wx = g.tv[6 * qq + 2 * u], wy = g.tv[6 * qq + 2 * u + 1];
-            zd Acomb = Mrr - (Mox * wx + Moy * wy) - (Msx * vx + Msy * vy) + M0 * (vx * wx + vy * wy);
-            zd val = (am_ * an) * (jw * Acomb + (Mq * 4.0) * inv_jw);
-            if (mode == 0) atomic_add_c<Zt>(Z, (size_t)em_ * ld + en, val);
-            else { ri[slot] = em_; ci[slot] = en; stc<double>(vv, slot, val); }
+            m[0] = half_sum(c0, mask);
+            const double rx_ = half_sum(crx, mask), ry_ = half_sum(cry, mask);
+            const double ax_ = half_sum(cax, mask), ay_ = half_sum(cay, mask);
+            m[5] = half_sum(crr, mask);
+            if (obs_rule) { m[1] = rx_; m[2] = ry_; m[3] = ax_; m[4] = ay_; }
+            else { m[1] = ax_; m[2] = ay_; m[3] = rx_; m[4] = ry_; }
+            if (kept && l == 0)
+                for (int c = 0; c < 6; ++c) kept[c] = m[c];
         }
+        const zd cA = x == 0 ? ldc<double>(tb.cA, t) : ldc<double>(tb.cAi, t);
+        const zd cq = x == 0 ? ldc<double>(tb.cq, t) : ldc<double>(tb.cqi, t);
+        s1 += cA * m[0]; sox += cA * m[1]; soy += cA * m[2]; ssx += cA * m[3]; ssy += cA * m[4]; srr += cA * m[5];
+        sq += cq * m[0];
     }
+    // minus the centroid-rule value of the far fill
+    {
+        zd ga, gq;
+        tab_kern<double>(tb, la, lb, cdist<double>(g.cent, p, qq), ga, gq);
+        const double wt = g.area[p] * g.area[qq];
+        const double ox = g.cent[2 * p], oy = g.cent[2 * p + 1], sx = g.cent[2 * qq], sy = g.cent[2 * qq + 1];
+        ga = ga * wt;
+        s1 -= ga; sox -= ga * ox; soy -= ga * oy; ssx -= ga * sx; ssy -= ga * sy; srr -= ga * (ox * sx + oy * sy);
+        sq -= gq * wt;
+    }
+    if (qcorr && l == 0) stc<double>(qcorr, i, sq);
+    // 3. one edge pair a lane
+    if (l >= 9) return;
+    const int s = l / 3, u = l - 3 * (l / 3);
+    const int em_ = g.te[3 * p + s], en = g.te[3 * qq + u];
+    const size_t slot = 9 * (size_t)i + l;
+    if (em_ < 0 || en < 0) {
+        if (mode == 2) { ri[slot] = -1; ci[slot] = 0; vv[2 * slot] = 0; vv[2 * slot + 1] = 0; }
+        return;
+    }
+    const double am = g.ta[3 * p + s], vx = g.tv[6 * p + 2 * s], vy = g.tv[6 * p + 2 * s + 1];
+    const double an = g.ta[3 * qq + u], wx = g.tv[6 * qq + 2 * u], wy = g.tv[6 * qq + 2 * u + 1];
+    // int (r - v).(r' - w) G_A and int G_q, from the moments
+    const zd vecA = srr - (sox * wx + soy * wy) - (ssx * vx + ssy * vy) + s1 * (vx * wx + vy * wy);
+    const zd val = (am * an) * (mk<double>(0, w) * vecA + (sq * 4.0) * mk<double>(0, -1.0 / w));
+    if (mode == 0) add_to_z<Zt>(Z, (size_t)em_ * ld + en, val);
+    else { ri[slot] = em_; ci[slot] = en; stc<double>(vv, slot, val); }
 }
 
 // ---- near pairs (mom25d_core.cpp:1216-1263): brute force over all pairs, rows in order -------------------------------
@@ -614,12 +639,12 @@ extern "C" int m25_near(int mode, void *d_Z, long ld, int single, int *d_ri, int
     M25_REQUIRE(mode != 2 || (d_ri && d_ci && d_vv), "m25_near: mode 2 needs ri, ci, vv");
     if (n == 0) return M25_OK;
     int *err = m25_dev_err_word();
-    long blocks = (n + 127) / 128;
+    const long blocks = (16 * n + 255) / 256;             // 16 lanes a pair
     if (single)
-        k_near<float><<<blocks, 128, 0, S(stream)>>>(mode, (float *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
+        k_near<float><<<blocks, 256, 0, S(stream)>>>(mode, (float *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
                                                      stat_ready, *g, *tb, *q, d_P, d_Q, n, w, err);
     else
-        k_near<double><<<blocks, 128, 0, S(stream)>>>(mode, (double *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
+        k_near<double><<<blocks, 256, 0, S(stream)>>>(mode, (double *)d_Z, ld, d_ri, d_ci, d_vv, d_qcorr, d_stat,
                                                       stat_ready, *g, *tb, *q, d_P, d_Q, n, w, err);
     M25_LAUNCH_CHECK("k_near");
     return M25_OK;
