@@ -14,7 +14,7 @@ for chains, fans and quadrature), so its compiled core and our kernels read iden
 """
 import numpy as np
 
-from .board import RWG, BAR3, BAR6, W3, W6, quad_pts, ViaPort, GapPort
+from .board import RWG, BAR3, BAR6, W3, W6, quad_pts, ViaPort, GapPort, LinePort
 
 
 class Geometry:
@@ -40,6 +40,7 @@ class Geometry:
         self._vias()
         self.ports = list(board.ports)
         self.N = self.Ne + self.Nv
+        self._port_edges()
 
     # ---- fast.py:377-406 ------------------------------------------------------------------------------------------
     def _pack(self):
@@ -145,19 +146,45 @@ class Geometry:
             tab[self.lidx[a], self.lidx[b]] = tab[self.lidx[b], self.lidx[a]] = i
         return tab
 
-    # ---- sim.py:988-1005: excitation and port currents --------------------------------------------------------------
+    # ---- sim.py:706-726, 988-1007: the ports' edges, excitation and port currents -----------------------------------
     def _port_chain(self, p):
         return next(n for n, (v, _, _) in enumerate(self.chains) if v is p.via)
 
-    def gap_edges(self, p, tol=None):
-        """sim.py:695-705: the edges on a gap port's transverse line, with their sign along the port direction."""
+    def line_edges(self, lp, s=0.0, tol=None):
+        """sim.py:695-705: the edges on the transverse line at distance s from lp's centre along its direction,
+        within its width, on its interface; with their sign along the direction."""
         r = self.rwg
         tol = tol or 1e-3 * self.dmax
-        e0, e1 = r.ends[:, 0] - p.c, r.ends[:, 1] - p.c
-        on = (np.abs(e0 @ p.d) < tol) & (np.abs(e1 @ p.d) < tol) & (self.edge_layer == p.layer)
-        on &= (np.abs(e0 @ p.t) <= p.w / 2 + tol) & (np.abs(e1 @ p.t) <= p.w / 2 + tol)
+        o = lp.c + lp.d * s
+        e0, e1 = r.ends[:, 0] - o, r.ends[:, 1] - o
+        on = (np.abs(e0 @ lp.d) < tol) & (np.abs(e1 @ lp.d) < tol) & (self.edge_layer == lp.layer)
+        on &= (np.abs(e0 @ lp.t) <= lp.w / 2 + tol) & (np.abs(e1 @ lp.t) <= lp.w / 2 + tol)
         idx = np.nonzero(on)[0]
-        return idx, np.sign(r.nrm[idx] @ p.d)
+        return idx, np.sign(r.nrm[idx] @ lp.d)
+
+    def gap_edges(self, p, tol=None):
+        """The edges of a gap port's (or a lumped element's, or a wave port's source) transverse line."""
+        return self.line_edges(p, 0.0, tol)
+
+    def _port_edges(self):
+        """sim.py:706-726: each port's source edges, and a wave port's sample positions and cut edges."""
+        self.samples, self.cuts, self.gaps = [], [], []
+        for p in self.ports:
+            if isinstance(p, ViaPort):
+                self.samples.append(None); self.cuts.append(None); self.gaps.append(None)
+                continue
+            gap = self.gap_edges(p)
+            if not len(gap[0]):
+                raise ValueError(f"port {p.name}: no mesh edges on the gap line")
+            self.gaps.append(gap)
+            if isinstance(p, LinePort):
+                s = p.sample_positions(self.dmax)
+                cuts = [self.line_edges(p, x) for x in s]
+                if not all(len(c[0]) for c in cuts):
+                    raise ValueError(f"port {p.name}: a sample cut off the conductor")
+                self.samples.append(s); self.cuts.append(cuts)
+            else:
+                self.samples.append(None); self.cuts.append(None)
 
     def excitation(self):
         E = np.zeros((self.N, len(self.ports)), complex)
@@ -165,30 +192,66 @@ class Geometry:
             if isinstance(p, ViaPort):
                 E[self.Ne + self._port_chain(p), j] = p.sign
             else:
-                idx, sig = self.gap_edges(p)
+                idx, sig = self.gaps[j]
                 E[idx, j] = sig * self.rwg.l[idx]
         return E
 
+    def port_rows(self):
+        """Every row of I that S needs: the via ports' chains, the gap ports' edges, the wave ports' cut edges."""
+        rows = []
+        for j, p in enumerate(self.ports):
+            if isinstance(p, ViaPort):
+                rows.append([self.Ne + self._port_chain(p)])
+            elif isinstance(p, LinePort):
+                rows += [idx for idx, _ in self.cuts[j]]
+            else:
+                rows.append(self.gaps[j][0])
+        return np.unique(np.concatenate(rows).astype(np.int64)) if rows else np.zeros(0, np.int64)
+
     def port_currents(self, I):
-        """(nports, ncols): each port's current for every excitation column (sim.py:997-1003)."""
+        """(nports, ncols): each port's current at its source for every excitation column (sim.py:997-1003)."""
         out = np.zeros((len(self.ports), I.shape[1]), complex)
         for j, p in enumerate(self.ports):
             if isinstance(p, ViaPort):
                 out[j] = p.sign * I[self.Ne + self._port_chain(p)]
             else:
-                idx, sig = self.gap_edges(p)
+                idx, sig = self.gaps[j]
                 out[j] = ((sig * self.rwg.l[idx])[:, None] * I[idx]).sum(0)
         return out
 
-    def sparams_from_currents(self, I):
-        """sim.py:1045-1092 for lumped ports: A = (V + zc I) / (2 sqrt zc), B = (V - zc I) / (2 sqrt zc),
-        S = B A^-1, V the unit EMF of each excitation column."""
+    def cut_currents(self, I, j):
+        """(n_cuts, ncols): the currents through wave port j's sample cuts (sim.py:1005-1007)."""
+        l = self.rwg.l
+        return np.array([((sig * l[idx])[:, None] * I[idx]).sum(0) for idx, sig in self.cuts[j]])
+
+    def sparams_from_currents(self, I, f=None, info=None):
+        """S from the currents of the excitation columns (sim.py:1045-1092): a lumped (via or gap) port's waves
+        A = (V + zc I) / (2 sqrt zc), B = (V - zc I) / (2 sqrt zc), V the unit EMF of each column; a wave port's
+        from the forward and backward waves fitted on its feed (ports.wave_port_waves); S = B A^-1, made reciprocal
+        when there are wave ports (ports.balance). info (a dict), where given, gets gamma, the fit residuals and
+        the ports' scales."""
+        from .ports import balance, wave_port_waves
         n = len(self.ports)
         Ip = self.port_currents(I)
         Ap, Bp = np.zeros((n, n), complex), np.zeros((n, n), complex)
+        gam, resid, low = np.full(n, np.nan + 0j), np.zeros(n), []
         for i, p in enumerate(self.ports):
-            if not isinstance(p, (ViaPort, GapPort)):
-                raise NotImplementedError("wave ports are outside the hot path")
-            Vp = np.eye(n)[i]
-            Ap[i], Bp[i] = (Vp + p.zc * Ip[i]) / (2 * np.sqrt(p.zc)), (Vp - p.zc * Ip[i]) / (2 * np.sqrt(p.zc))
-        return Bp @ np.linalg.inv(Ap)
+            if getattr(p, 'zc_fn', None) is not None and f is not None:
+                p.zc = float(p.zc_fn(f))
+            if isinstance(p, LinePort):
+                Ap[i], Bp[i], gam[i], resid[i], span = wave_port_waves(p, self.samples[i], self.cut_currents(I, i), f)
+                if span < 0.4:
+                    low.append(p.name)
+            elif isinstance(p, (ViaPort, GapPort)):
+                Vp = np.eye(n)[i]
+                Ap[i], Bp[i] = (Vp + p.zc * Ip[i]) / (2 * np.sqrt(p.zc)), (Vp - p.zc * Ip[i]) / (2 * np.sqrt(p.zc))
+            else:
+                raise NotImplementedError(f"port {getattr(p, 'name', p)}: via, gap or wave (LinePort) ports")
+        S = Bp @ np.linalg.inv(Ap)
+        wave = np.array([isinstance(p, LinePort) for p in self.ports])
+        scale = np.ones(n)
+        if wave.any() and n > 1:
+            S, scale = balance(S, ~wave)
+        if info is not None:
+            info.update(gamma=gam, resid=resid, scale=scale, low_span=low)
+        return S

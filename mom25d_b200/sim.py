@@ -4,8 +4,9 @@ Simulation(...).sparams(f) / .currents(f, E) / .excitation(), solved on one GPU 
 solver (operator.DirectSolver).
 
 Differences from the reference's Simulation, all outside the hot path: meshes are built by this package's
-Manhattan tensor mesher (board.py) from rectangles, not by the shapely mesher; ports are via ports or gap ports
-(lumped); no wave ports, lumped elements, metal loss, frills, slots, quads or loop/tree basis.
+Manhattan tensor mesher (board.py) from rectangles, not by the shapely mesher, so feeds and ports run along x or y;
+ports are via ports, gap ports (lumped) or wave ports on a straight feed (LinePort), with series lumped elements
+and conductor loss (extras.py); no differential ports, frills, slots, quad cells or loop/tree basis.
 
 Precision policy (fast.py:704-850, 1075-1084): 'double' (the drop-in, matches the reference's complex128 path),
 'mixed' (complex64 fill and LU refined in double by GMRES), 'auto' (mixed above MIXED_MIN_N unknowns). A mixed
@@ -17,7 +18,7 @@ import time
 import numpy as np
 import torch
 
-from .board import Board, LayerStack, Via, ViaPort, GapPort, mesh_layers
+from .board import Board, LayerStack, Via, ViaPort, GapPort, LinePort, mesh_layers, port_lines
 from .geometry import Geometry
 from .operator import DirectSolver, SolveFailed
 
@@ -53,13 +54,8 @@ class Simulation:
             if stack is None or shapes is None:
                 raise ValueError("Simulation needs (stack, shapes) or board=")
             vias = list(vias) + [p.via for p in ports if isinstance(p, ViaPort) and p.via not in vias]
-            lines = {}
-            for el in lumped:                             # along x: the cut is the line x = c.x; along y: y = c.y
-                xl, yl = lines.setdefault(el.layer, ([], []))
-                if abs(el.lp.d[0]) >= abs(el.lp.d[1]):
-                    xl.append(float(el.lp.c[0]))
-                else:
-                    yl.append(float(el.lp.c[1]))
+            # the cut lines of gap ports and lumped elements, a wave port's gap and sample cuts (sim.py:424-440)
+            lines = port_lines(ports, lumped, dmax)
             nodes, tris, tl = mesh_layers(stack, shapes, dmax, ncross=ncross, grade=grade, w_ref=w_ref, vias=vias,
                                           lines=lines)
             board = Board(stack, nodes, tris, tl, list(vias), list(ports), dmax, near_fac, 'simulation',
@@ -117,33 +113,21 @@ class Simulation:
                                                           f"iters {self.fast.iters}")
         return I
 
-    def port_rows(self):
-        """The rows of I that the lumped ports read, with their weights (sim.py:997-1003)."""
-        rows, wts, which = [], [], []
-        for j, p in enumerate(self.ports):
-            if isinstance(p, ViaPort):
-                rows.append(self.Ne + self.geo._port_chain(p)); wts.append(p.sign); which.append(j)
-            else:
-                idx, sig = self.geo.gap_edges(p)
-                rows += idx.tolist(); wts += (sig * self.geo.rwg.l[idx]).tolist(); which += [j] * len(idx)
-        return np.array(rows), np.array(wts), np.array(which)
-
     def sparams(self, f, keep=False):
-        """S at f (sim.py:1045-1092, lumped ports): the excitation copied to the device, the solve, the port
-        currents gathered there and read back."""
+        """S at f (sim.py:1045-1092): the excitation copied to the device, the solve, the rows of the currents
+        that the ports read gathered there and read back, the waves and S on the host (lumped ports' voltages and
+        currents; wave ports' fitted feed waves, then the reciprocity balance)."""
         E = self.excitation()
         I = self.currents(f, E)
-        rows, wts, which = self.port_rows()
-        Ir = I[torch.as_tensor(rows, device=I.device)].cpu().numpy()          # the port rows only
-        n = len(self.ports)
-        Ip = np.zeros((n, I.shape[1]), complex)
-        np.add.at(Ip, which, wts[:, None] * Ir)
-        Ap, Bp = np.zeros((n, n), complex), np.zeros((n, n), complex)
-        for i, p in enumerate(self.ports):
-            Vp = np.eye(n)[i]
-            Ap[i], Bp[i] = (Vp + p.zc * Ip[i]) / (2 * np.sqrt(p.zc)), (Vp - p.zc * Ip[i]) / (2 * np.sqrt(p.zc))
-        S = Bp @ np.linalg.inv(Ap)
-        self.last = dict(f=f, I=I if keep else None, A=Ap, B=Bp)
+        rows = self.geo.port_rows()
+        Ih = np.zeros((self.N, I.shape[1]), complex)
+        Ih[rows] = I[torch.as_tensor(rows, device=I.device)].cpu().numpy()      # the port rows only
+        info = {}
+        S = self.geo.sparams_from_currents(Ih, f, info)
+        self.last = dict(f=f, I=I if keep else None, **info)
+        for name in info.get('low_span', []):
+            self.log.note(f"WARNING {f / 1e9:.2f} GHz port {name}: its feed samples span less than 0.4 rad - wave "
+                          f"separation unreliable (lengthen the straight feed or use a via / gap port)")
         return S
 
     def sweep(self, freqs):
