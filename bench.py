@@ -220,6 +220,7 @@ def run_gpu(args, rank, world):
     def cold():
         """A sweep starts with no kept LUs and nothing learnt (the warm-up leaves some)."""
         ds.kept, ds.reach, ds.t_iter, ds.mixed_failed = [], float(np.log(2.0)), None, 0.0
+        ds.kept64, ds.t_iter64 = None, None
 
     for i in range(args.warmup):
         step_device(mine[i % len(mine)], 'mixed')

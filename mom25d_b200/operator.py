@@ -38,6 +38,12 @@ PREDICT_AFTER = 6            # iterations after which a fresh factor's refinemen
 MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
 REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
 REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most
+REUSE_GIVE_UP = (8, 10.0)    # a reused factor's GMRES ends once, after this many steps, its last steps' rate cannot
+                             # bring the residual within this factor of the tolerance by its cap (a fresh LU follows)
+DOUBLE_REACH = float(np.log(1.5))  # |ln f / f0| within which the kept double factor preconditions a double solve
+
+
+SMALL = 1e-300
 
 
 class SolveFailed(RuntimeError):
@@ -65,6 +71,9 @@ class DirectSolver:
         self.last_lu_ms = self.last_lu_c64_ms = None
         self.attempts = []                 # reused-LU attempts: (f, f0, cap, iterations, converged, residual)
         self.extras = None                 # extras.ExtraBlocks: lumped elements, conductor loss (fast.py:628-641)
+        self.kept64 = None                 # (f, factor record, dsc, seconds): the last double LU made next to a
+                                           # complex64 failure, preconditioning the double solves near it
+        self.t_iter64 = None
 
     # ---- buffers kept across frequencies ---------------------------------------------------------------------------
     def _buf(self, name, shape, dtype):
@@ -77,6 +86,38 @@ class DirectSolver:
     def _getrf_work(self, n, single):
         nbytes = int(lib().m25_getrf_workspace(c_int(n), c_int(1 if single else 0)))
         return self._buf('getrf_work_%d' % single, (nbytes,), torch.uint8)
+
+    # ---- device memory ------------------------------------------------------------------------------------------------
+    def release(self):
+        """Drops every per-frequency buffer (Z, its complex64 copies and factors, kept LUs, workspaces, Krylov
+        bases, tables); what stays is the per-board state (resident_bytes). The memory goes back to torch's
+        caching allocator."""
+        self._work.clear()
+        self.kept, self.kept64 = [], None
+        for name in ('aux', 'tabs', 'vias', 'ri', 'ci', 'vv', 'Bv', 'Cv'):
+            if hasattr(self, name):
+                delattr(self, name)
+        if self.extras is not None:
+            self.extras._vals, self.extras._vals_f = None, None
+
+    def resident_bytes(self):
+        """Device bytes the board's state holds between requests: mesh, quadrature, near pairs and their kept
+        analytic moments, the via index lists."""
+        seen, total = set(), 0
+        for t in list(self.dg.__dict__.values()) + list(self.dg.t.values()) + list(self.dg.tq.values()) + \
+                [g[k] for g in getattr(self.dg, 'groups', []) for k in ('m', 'n', 'dd')]:
+            if torch.is_tensor(t) and t.is_cuda and t.data_ptr() not in seen:
+                seen.add(t.data_ptr())
+                total += t.numel() * t.element_size()
+        return total
+
+    def held_bytes(self):
+        """Device bytes this solver holds now beyond its resident state (per-frequency buffers and kept factors)."""
+        total = sum(t.numel() * t.element_size() for t in self._work.values())
+        total += sum(k[1]['bytes'] for k in self.kept)
+        if self.kept64 is not None:
+            total += self.kept64[1]['Z'].numel() * 16 + self.kept64[1]['aux'].numel()
+        return total
 
     @property
     def s(self):
@@ -246,6 +287,8 @@ class DirectSolver:
         self.last_lu_ms = self.last_lu_c64_ms = None
         if precision == 'mixed' and f <= MIXED_RETRY * self.mixed_failed:
             precision = 'double'                          # fast.py:740: near a failure, double
+            if self._hybrid_fits():
+                return self._solve_double_near(f, E)
         if precision == 'mixed' and self._hybrid_fits():
             return self._solve_kept(f, E)
         self.last_path = precision
@@ -375,7 +418,7 @@ class DirectSolver:
             M = lambda R: self._timed('refine_precond', lambda: self._scale(self._solve_c64(rec, self._scale(R, rows=r)),
                                                                               rows=r))
             e0, t = self._mark(), time.perf_counter()
-            Y, ok, rel = self.refine(A, B, M, cap)
+            Y, ok, rel = self.refine(A, B, M, cap, give_up=REUSE_GIVE_UP)
             self._learn_t_iter((time.perf_counter() - t) / max(1, max(self.iters, default=1)))
             self._reach_learn(abs(np.log(f / f0)), ok, self.iters, cap)
             self.attempts.append(dict(f=f, f0=f0, cap=cap, iters=max(self.iters, default=0), ok=ok, rel=rel))
@@ -401,16 +444,68 @@ class DirectSolver:
                 self.kept.append((f, rec, dsc, time.perf_counter() - t_fresh0))
             return self._scale(Y, rows=dsc)
         del rec, Z64
-        # the double LU of the same (equilibrated) Z, and double up to MIXED_RETRY x f (fast.py:1074-1084)
+        # the double LU of the same (equilibrated) Z, and double up to MIXED_RETRY x f (fast.py:1074-1084); that LU
+        # is kept to precondition the double solves near f (_solve_double_near)
         self.mixed_failed = max(self.mixed_failed, f)
         self.log.append(f"mixed precision did not converge at {f / 1e9:.4g} GHz (residual {rel:.1e}): double LU of the "
                         f"same Z, double up to {MIXED_RETRY * f / 1e9:.4g} GHz")
         self.last_path = 'double (after mixed)'
+        return self._double_fresh(f, Z, dsc, B, time.perf_counter())
+
+    def _double_fresh(self, f, Z, dsc, B, t0):
+        """A double LU of the equilibrated Z (in place) and its solve; the factor is kept (self.kept64), its memory
+        leaving the solver's work buffers."""
         ipiv = self._factor(Z, False)
-        t0 = self._mark()
+        e0 = self._mark()
         X = self._lu_solve(Z, ipiv, B, False)
-        self._t('solve', t0)
+        self._t('solve', e0)
+        rec = dict(Z=Z, aux=self.aux, ipiv=ipiv)
+        for name in ('Z', 'getrs_aux_0', 'ipiv'):         # the next fill and factor take new buffers
+            self._work.pop(name, None)
+        self.kept64 = (f, rec, dsc.clone(), time.perf_counter() - t0)
         return self._scale(X, rows=dsc)
+
+    def _solve_c128(self, rec, R):
+        """Z^-1 R with a kept double factor, R complex128 (N x k)."""
+        N, k = R.shape
+        X = R.clone()
+        check(lib().m25_getrs_aux(P(rec['Z']), c_long(N), c_int(N), c_int(0), P(rec['aux']), P(X), c_int(k), self.s),
+              'm25_getrs_aux')
+        return X
+
+    def _solve_double_near(self, f, E):
+        """A frequency the reference solves in double because the complex64 factor failed near it (fast.py:740):
+        GMRES on the dense double Z preconditioned by the double LU kept from the failure's neighbourhood (within
+        DOUBLE_REACH in |ln f / f0|, scaled by the equilibrations as kept complex64 LUs are), capped at what a
+        fresh double LU costs; a fresh double LU (then kept) where there is none or it does not converge."""
+        N = self.geo.N
+        t0 = time.perf_counter()
+        Z = self.impedance(f, 'double')
+        dsc = self._buf('dsc', (N,), torch.float64)
+        check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
+        dsc = dsc.clone()
+        B = self._scale(E, rows=dsc)
+        k = self.kept64
+        if k is not None and abs(np.log(f / k[0])) <= DOUBLE_REACH:
+            f0, rec, d0, t_fresh = k
+            r = (d0 / dsc).contiguous()
+            cap = int(np.clip(0.8 * t_fresh / max(self.t_iter64 or 0.04, 1e-6), *REUSE_ITER))
+            A = lambda V: self._timed('refine_matvec', lambda: self._dense(Z, V))
+            M = lambda R: self._timed('refine_precond', lambda: self._scale(self._solve_c128(rec, self._scale(R, rows=r)),
+                                                                              rows=r))
+            e0, t = self._mark(), time.perf_counter()
+            Y, ok, rel = self.refine(A, B, M, cap, give_up=REUSE_GIVE_UP)
+            it = max(1, max(self.iters, default=1))
+            self.t_iter64 = (time.perf_counter() - t) / it if self.t_iter64 is None else \
+                min(self.t_iter64, (time.perf_counter() - t) / it)
+            self._t('refine', e0)
+            self.attempts.append(dict(f=f, f0=f0, cap=cap, iters=max(self.iters, default=0), ok=ok, rel=rel,
+                                      double=True))
+            if ok:
+                self.last_path = 'reused double'
+                return self._scale(Y, rows=dsc)
+        self.last_path = 'double'
+        return self._double_fresh(f, Z, dsc, B, t0)
 
     def _learn_t_iter(self, t):
         """The time of one refinement iteration, which sets a reused LU's cap (fast.py:1019): the smallest seen, so
@@ -424,10 +519,11 @@ class DirectSolver:
         return out
 
     # ---- the refinement: batched right-preconditioned GMRES (fast.py:658-663, 1437-1500) -----------------------------
-    def refine(self, A, B, M, restart, stall=None, predict=True):
+    def refine(self, A, B, M, restart, stall=None, predict=True, give_up=None):
         """fast.py:658-663: GMRES to MIXED_RTOL, one cycle of at most `restart` iterations; (Y, converged, largest
         relative residual of B - A Y)."""
-        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, stall=stall, predict=predict)
+        Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, stall=stall, predict=predict,
+                                           give_up=give_up)
         R = B - A(Y)
         rn = np.sqrt(np.abs(self._dotc(R, R)))
         bn = np.sqrt(np.abs(self._dotc(B, B)))
@@ -435,7 +531,7 @@ class DirectSolver:
         self.residual = rel
         return Y, bool(np.isfinite(rel).all() and (rel <= 100 * MIXED_RTOL).all()), float(rel.max())
 
-    def gmres_batched(self, A, B, M, rtol=1e-6, restart=30, stall=None, predict=True):
+    def gmres_batched(self, A, B, M, rtol=1e-6, restart=30, stall=None, predict=True, give_up=None):
         """Right-preconditioned GMRES on A Y = B for the k columns of B at once, one cycle from Y = 0, the role of
         the reference's gmres_batched (fast.py:1437-1500) as its callers use it (maxiter 1, fast.py:1053):
 
@@ -467,6 +563,7 @@ class DirectSolver:
         steps = np.zeros(k, int)              # steps each column takes (its y has that many entries)
         done = np.zeros(k, bool)
         res = bn.copy()
+        hist = [bn.copy()]
         for j in range(restart):
             Zd[j].copy_(M(V[j]))
             W = A(Zd[j]).contiguous()
@@ -479,9 +576,14 @@ class DirectSolver:
             res[live] = np.abs(g[:, j + 1])
             steps[live] = j + 1
             done[live] |= res[live] <= rtol * bn[live]
+            hist.append(res.copy())
             if done.all():
                 break
             act = ~done
+            if give_up is not None and j + 1 >= give_up[0] and j + 1 < restart:
+                rate = (res[act] / np.maximum(hist[-4][act], SMALL)) ** (1.0 / 3)
+                if (res[act] * rate ** (restart - j - 1) > give_up[1] * rtol * bn[act]).any():
+                    break
             if stall is not None and j + 1 >= stall[0] and (res[act] > stall[1] * bn[act]).any():
                 break
             if stall is not None and predict and j + 1 >= PREDICT_AFTER:

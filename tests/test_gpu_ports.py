@@ -52,13 +52,13 @@ def test_line_char_xs_microstrip_is_physical():
     from mom25d_b200.ports import line_char_xs
     h, er, w = 0.8e-3, 4.4, 1.5e-3
     st = LayerStack([Layer(h, er, 0.0)])
-    f = np.array([1e9, 3e9])
-    gam, zc = line_char_xs(st, 1, w, f, dmax=0.4e-3)
+    f = np.array([3e9, 6e9])                              # (the cuts span enough phase for the fit: FIT_SPAN)
+    gam, zc = line_char_xs(st, 1, w, f, dmax=0.4e-3, length=24e-3)
     u = w / h                                             # Hammerstad-Jensen, zero thickness
     eeff = (er + 1) / 2 + (er - 1) / 2 * (1 + 10 / u) ** -0.555
     fu = 6 + (2 * np.pi - 6) * np.exp(-(30.666 / u) ** 0.7528)
     z0 = 60 / np.sqrt(eeff) * np.log(fu / u + np.sqrt(1 + (2 / u) ** 2))
     beta = 2 * np.pi * f / C0 * np.sqrt(eeff)
     assert np.all(np.abs(gam.imag / beta - 1) < 0.05), gam.imag / beta
-    assert np.all(np.abs(zc.real / z0 - 1) < 0.1), (zc, z0)
+    assert np.all(np.abs(zc.real / z0 - 1) < 0.15), (zc, z0)
     assert np.all(gam.real >= 0)
