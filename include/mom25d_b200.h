@@ -153,6 +153,13 @@ int m25_via_pairs(const int *d_pm, const int *d_pn, const double *d_dd, int np, 
  * tables tbf (the mixed-precision fill), else complex128 from tb. */
 int m25_fill_far(void *d_Z, long ld, int single, const m25_mesh *g, const m25_tables *tb, const m25_tables_f *tbf,
                  double w, void *stream);
+/* The far fill of several frequencies of one board in one launch (the reference fills one frequency a call,
+ * fill_far, mom25d_core.cpp:132-173; this serves a batched sweep): d_Zs a device array of nf matrix pointers
+ * (row-major N x ld each, complex128 or complex64 by `single`), d_tables a device array of nf m25_tables
+ * (complex128) or m25_tables_f (complex64) structs, d_w the nf angular frequencies on the device. Each Z gets
+ * exactly what m25_fill_far writes for its frequency. */
+int m25_fill_far_multi(void *const *d_Zs, long ld, int single, const m25_mesh *g, const void *d_tables,
+                       const double *d_w, int nf, void *stream);
 /* The far field for row / column edge lists: out complex128[nr*nc] (far_block, mom25d_core.cpp:176-211). */
 int m25_far_block(const int *d_rows, int nr, const int *d_cols, int nc, double *d_out, const m25_mesh *g,
                   const m25_tables *tb, double w, void *stream);
@@ -241,6 +248,13 @@ size_t m25_getrf_workspace(int n, int single);
  * only): trailing updates on the tensor cores as 3xTF32 products. */
 int m25_getrf(void *d_A, long lda, int n, int *d_ipiv, int single, int tf32, void *d_work, size_t work_bytes,
               void *stream);
+/* The LU's tile parameters by matrix size (no counterpart in the reference: LAPACK picks its own blocking): up to
+ * 32 entries (n, outer panel width nb2 = 64..256 in steps of 64, cooperative panel blocks), as the autotuner
+ * (mom25d_b200/tune.py) finds them on this GPU; a factorisation of size n takes the entry with the largest n at or
+ * below its own. count 0 restores the defaults (256, min(SMs, 32)). The environment variables M25_NB2 and
+ * M25_PANEL_BLOCKS override both. m25_get_lu_tuning: what a factorisation of size n uses. */
+int m25_set_lu_tuning(const int *h_n, const int *h_nb2, const int *h_blocks, int count);
+int m25_get_lu_tuning(int n, int *nb2, int *blocks);
 /* Solves Z X = B with the factor of Z^T (lu_solve(..., trans=1)); B (row-major n x nrhs, complex in the factor's
  * precision) overwritten by X. */
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);

@@ -57,7 +57,26 @@ def lib():
         L.m25_pair_record_bytes.restype = ctypes.c_size_t
         L.m25_launch_count.restype = ctypes.c_longlong
         _lib = L
+        apply_tuning(L)
     return _lib
+
+
+def apply_tuning(L, path=None):
+    """The autotuner's LU parameters (tune.py, tuning_b200.json beside this file), where that file exists and was
+    made on a device with this SM count; otherwise the library's defaults stay."""
+    import json
+    path = path or os.path.join(HERE, 'tuning_b200.json')
+    if not os.path.exists(path):
+        return False
+    doc = json.load(open(path))
+    try:
+        if torch.cuda.is_available() and torch.cuda.get_device_properties(0).multi_processor_count != doc.get('sms'):
+            return False
+    except Exception:
+        pass
+    ent = doc.get('entries', [])
+    arr = lambda k: (ctypes.c_int * max(1, len(ent)))(*[int(e[k]) for e in ent])
+    return L.m25_set_lu_tuning(arr('n'), arr('nb2'), arr('blocks'), len(ent)) == 0
 
 
 def check(rc, what=''):

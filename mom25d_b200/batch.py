@@ -8,10 +8,13 @@ The workload is the stub filter board (board.stub_filter_board: three layers 0.2
 40 mm long with an open quarter-wave stub at 2.4 GHz, dmax 0.2 mm, a via port at each line end) at
 linspace(fmin, fmax, freqs).
 
-  - batched: all frequencies are present at the start and go through the serving loop (serve.Server): each slot
-    has its own CUDA stream, host thread and solver, so one frequency's panel factorisation, triangular solves and
-    host synchronisations overlap the others' tensor-core updates. Kept-LU reuse is off (each frequency's result
-    does not depend on the others');
+  - batched: the Green tables of every frequency are built and kept on the device, and the far part of every
+    frequency's double Z is filled by one launch (m25_fill_far_multi, grid z = frequency; in chunks where the
+    matrices of all frequencies would not fit); then all frequencies are present at the start and go through the
+    serving loop (serve.Server), each with its prefilled Z: each slot has its own CUDA stream, host thread and
+    solver, which adds the near field and via border, factors and refines, so one frequency's panel
+    factorisation, triangular solves and host synchronisations overlap the others' tensor-core updates. Kept-LU
+    reuse is off (each frequency's result does not depend on the others');
   - sequential mixed: the reference's sweep (fast.py:996-1118) on one stream, kept complex64 LUs reused within the
     learnt reach;
   - FP64: the drop-in path, one frequency after another (each its own complex128 fill and LU).
@@ -33,11 +36,55 @@ def sweep_requests(key, freqs):
     return [Request(i, key, f, 0.0) for i, f in enumerate(freqs)]
 
 
-def batched_sweep(server, key, freqs):
-    """All frequencies through the server at once: (S list in frequency order, wall seconds, requests)."""
-    reqs = sweep_requests(key, freqs)
+def fill_far_sweep(geo, dg, freqs, stream=None):
+    """The far part of the double Z at every frequency in one launch (m25_fill_far_multi): each frequency's Green
+    tables (device.DeviceTables) built and kept, one N x N complex128 Z a frequency. Returns (Zs, tables)."""
+    import ctypes
+    import torch
+    from ._lib import P, check, lib, stream_ptr
+    from .device import DeviceTables
+    N = geo.N
+    tabs = [DeviceTables(dg, f, stream=stream) for f in freqs]
+    Zs = [torch.empty((N, N), dtype=torch.complex128, device='cuda') for _ in freqs]
+    ptrs = torch.tensor([Z.data_ptr() for Z in Zs], dtype=torch.int64, device='cuda')
+    raw = b''.join(ctypes.string_at(ctypes.addressof(t.tables), ctypes.sizeof(t.tables)) for t in tabs)
+    d_tb = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to('cuda')
+    d_w = torch.tensor([2 * np.pi * f for f in freqs], dtype=torch.float64, device='cuda')
+    check(lib().m25_fill_far_multi(P(ptrs), ctypes.c_long(N), ctypes.c_int(0), ctypes.byref(dg.mesh), P(d_tb), P(d_w),
+                                   ctypes.c_int(len(freqs)), stream_ptr(stream)), 'm25_fill_far_multi')
+    (stream or torch.cuda.current_stream()).synchronize()
+    return Zs, tabs
+
+
+def batched_sweep(server, key, freqs, multi=True):
+    """All frequencies through the server at once: (S list in frequency order, wall seconds, requests). multi: the
+    far part of every frequency's Z filled first by one launch (in chunks of what fits), the requests carrying
+    their Z; else each request fills its own."""
     t = time.perf_counter()
-    server.run(reqs)
+    if not multi:
+        reqs = sweep_requests(key, freqs)
+        server.run(reqs)
+    else:
+        import torch
+        from .device import DeviceGeometry
+        geo = server._geometry(key)
+        dg = getattr(server, '_fill_dg', {}).get(key)
+        if dg is None:
+            dg = DeviceGeometry(geo)
+            server._fill_dg = {key: dg}
+        free, _ = torch.cuda.mem_get_info()
+        per = 16.0 * geo.N * geo.N
+        room = 0.8 * free - server.slots * (server.footprint(key) + 2e9)
+        chunk = max(1, min(len(freqs), int(room // per)))
+        reqs = []
+        for c0 in range(0, len(freqs), chunk):
+            part = [float(f) for f in freqs[c0:c0 + chunk]]
+            Zs, tabs = fill_far_sweep(geo, dg, part)
+            rq = [Request(c0 + i, key, f, 0.0, far=Z) for i, (f, Z) in enumerate(zip(part, Zs))]
+            del Zs
+            server.run(rq)
+            reqs += rq
+            del rq, tabs
     wall = time.perf_counter() - t
     bad = [r for r in reqs if r.error is not None]
     if bad:
@@ -72,6 +119,7 @@ def run(board, freqs, slots=6, fp64_count=None, sequential_mixed=True):
     # warm-up: a solve on every slot (kernels loaded, solvers, streams and buffers built)
     batched_sweep(srv, key, [freqs[len(freqs) // 2]] * slots)
     S_b, wall_b, reqs = batched_sweep(srv, key, freqs)
+    del srv._fill_dg
     out = dict(workload=f"{key}: N={N} unknowns, {len(freqs)} frequencies linspace({freqs[0] / 1e9:.4g}, "
                         f"{freqs[-1] / 1e9:.4g} GHz)", unknowns=N, frequencies=len(freqs), slots=slots,
                batched=dict(solves_per_s=round(len(freqs) / wall_b, 3), wall_s=round(wall_b, 3),

@@ -66,7 +66,7 @@ struct EdgeHalves { int p[2]; int lt[2]; double a[2], dx[2], dy[2]; };
 #define FF_SMEM (48 * 1024)
 
 template <typename R, typename TB>
-__global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB tb, double w)
+__device__ __forceinline__ void fill_far_tile(R *Z, long ld, const m25_mesh &g, const TB &tb, double w)
 {
     typedef cpx<R> C;
     extern __shared__ __align__(16) unsigned char ff_raw[];
@@ -158,6 +158,23 @@ __global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB 
             }
         stc<R>(Z, (size_t)m * ld + n, v);
     }
+}
+
+template <typename R, typename TB>
+__global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB tb, double w)
+{
+    fill_far_tile<R, TB>(Z, ld, g, tb, w);
+}
+
+// Several frequencies of one board in one launch: grid z is the frequency, each with its own Z, tables and w (the
+// batched sweep: the far part of every frequency's Z, the tables of all of them resident).
+template <typename R, typename TB>
+__global__ void __launch_bounds__(256) k_fill_far_multi(R *const *Zs, long ld, m25_mesh g, const TB *tbs,
+                                                        const double *ws)
+{
+    const int f = blockIdx.z;
+    const TB tb = tbs[f];
+    fill_far_tile<R, TB>(Zs[f], ld, g, tb, ws[f]);
 }
 
 // far_block (mom25d_core.cpp:176-211): arbitrary row / column edge lists, complex128 out
@@ -615,6 +632,28 @@ extern "C" int m25_fill_far(void *d_Z, long ld, int single, const m25_mesh *g, c
         k_fill_far<double, m25_tables><<<grid, block, FF_SMEM, S(stream)>>>((double *)d_Z, ld, *g, *tb, w);
     }
     M25_LAUNCH_CHECK("k_fill_far");
+    return M25_OK;
+}
+
+extern "C" int m25_fill_far_multi(void *const *d_Zs, long ld, int single, const m25_mesh *g, const void *d_tables,
+                                  const double *d_w, int nf, void *stream)
+{
+    M25_REQUIRE(d_Zs && g && d_tables && d_w && ld >= g->Ne && nf >= 1 && nf <= 65535,
+                "m25_fill_far_multi: Zs, g, tables, w, ld >= Ne, 1 <= nf <= 65535");
+    if (g->Ne == 0) return M25_OK;
+    dim3 grid((g->Ne + 31) / 32, (g->Ne + 31) / 32, nf), block(32, 8);
+    if (single) {
+        M25_CHECK(cudaFuncSetAttribute(k_fill_far_multi<float, m25_tables_f>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, FF_SMEM));
+        k_fill_far_multi<float, m25_tables_f><<<grid, block, FF_SMEM, S(stream)>>>(
+            (float *const *)d_Zs, ld, *g, (const m25_tables_f *)d_tables, d_w);
+    } else {
+        M25_CHECK(cudaFuncSetAttribute(k_fill_far_multi<double, m25_tables>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, FF_SMEM));
+        k_fill_far_multi<double, m25_tables><<<grid, block, FF_SMEM, S(stream)>>>(
+            (double *const *)d_Zs, ld, *g, (const m25_tables *)d_tables, d_w);
+    }
+    M25_LAUNCH_CHECK("k_fill_far_multi");
     return M25_OK;
 }
 

@@ -14,6 +14,9 @@
 //                  (umma.cu) for complex64 with tf32 on.
 #include <cooperative_groups.h>
 #include <type_traits>
+#include <algorithm>
+#include <mutex>
+
 #include "common.cuh"
 
 static inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
@@ -74,37 +77,6 @@ __device__ __forceinline__ bool ll_wait(const unsigned long long *p, int stride,
     }
 }
 
-#ifdef M25_PANEL_TIMING
-// per-phase SM cycles of the panel kernel (thread 0 of every block), summed over blocks and launches, with the
-// count of block-launches in the last slot: a measurement build only
-__device__ unsigned long long g_panel_phase[8];
-#define PANEL_T(q)                                                                                                     \
-    do {                                                                                                               \
-        if (threadIdx.x == 0) {                                                                                        \
-            const long long t_ = clock64();                                                                            \
-            pt_acc[q] += t_ - pt_last;                                                                                 \
-            pt_last = t_;                                                                                              \
-        }                                                                                                              \
-    } while (0)
-#define PANEL_T_BEGIN                                                                                                  \
-    unsigned long long pt_acc[7] = {0, 0, 0, 0, 0, 0, 0};                                                              \
-    long long pt_last = clock64()
-#define PANEL_T_END                                                                                                    \
-    do {                                                                                                               \
-        if (threadIdx.x == 0) {                                                                                        \
-            for (int q_ = 0; q_ < 7; ++q_) atomicAdd(&g_panel_phase[q_], pt_acc[q_]);                                  \
-            atomicAdd(&g_panel_phase[7], 1ull);                                                                        \
-        }                                                                                                              \
-    } while (0)
-extern "C" int m25_panel_timing(unsigned long long *out8)
-{
-    return cudaMemcpyFromSymbol(out8, g_panel_phase, sizeof(unsigned long long) * 8) == cudaSuccess ? 0 : 1;
-}
-#else
-#define PANEL_T(q)
-#define PANEL_T_BEGIN
-#define PANEL_T_END
-#endif
 
 #define PANEL_NONE 0x7fffffff
 #define LL_REC 32             // words a candidate record (256 bytes: polled by every block, one record a line pair)
@@ -150,14 +122,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
     __shared__ R sv[NWARP], sv2[NWARP];
     __shared__ int si[NWARP], si2[NWARP], sw2[NWARP];
     __shared__ int s_fail;
-    PANEL_T_BEGIN;
     for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
         int c = e / nr, i = e % nr;
         Ps[c * cs + i] = ldc<R>(A, (size_t)(k0 + c) * lda + r0 + i);
     }
     if (tid == 0) s_fail = 0;
     __syncthreads();
-    PANEL_T(0);
     R best = -1;                                          // this thread's candidate for column 0
     int bi = PANEL_NONE;
     for (int i = tid; i < nr; i += PANEL_THREADS) {
@@ -172,7 +142,6 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         warp_argmax(best, bi);
         if (lane == 0) { sv[wid] = best; si[wid] = bi; }
         __syncthreads();                                  // (column j is complete for every row >= col)
-        PANEL_T(1);
         best = sv[0]; bi = si[0];
         for (int w = 1; w < NWARP; ++w)
             if (sv[w] > best || (sv[w] == best && si[w] < bi)) { best = sv[w]; bi = si[w]; }
@@ -253,7 +222,6 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         }
         if (lane == 0) { sv2[wid] = bv; si2[wid] = brow; sw2[wid] = bw; }
         __syncthreads();                                  // (and the deferred update is complete)
-        PANEL_T(2);
         if (s_fail) return;
         bv = sv2[0]; brow = si2[0]; bw = sw2[0];
         for (int w = 1; w < NWARP; ++w)
@@ -284,7 +252,6 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
             }
         }
         __syncthreads();
-        PANEL_T(3);
         if (s_fail) return;
         // (6) rows col and p interchanged (whole panel rows), column j scaled by 1 / pivot, column j + 1 updated
         // (the rest of this column's update is deferred to the next column's step 3); the next candidates
@@ -320,15 +287,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                 if (v > best) { best = v; bi = row; }
             }
         }
-        PANEL_T(4);
     }
     __syncthreads();
     for (int e = tid; e < nr * jb; e += PANEL_THREADS) {
         int c = e / nr, i = e % nr;
         stc<R>(A, (size_t)(k0 + c) * lda + r0 + i, Ps[c * cs + i]);
     }
-    PANEL_T(5);
-    PANEL_T_END;
 }
 
 // The same with the rows in global memory (when a block's rows do not fit in shared memory).
@@ -1333,6 +1297,57 @@ int lu_streams(LuStreams *out)
 }
 }  // namespace
 
+// ---- the LU's tile parameters by matrix size (set by the autotuner, mom25d_b200.tune) --------------------------------
+// Entries (n, outer panel width, panel blocks), sorted by n; a factorisation of size n takes the entry with the
+// largest n at or below its own (the first entry below all of them). Without entries: NB2 and min(SMs, 32).
+namespace {
+struct LuTuning { int n, nb2, blocks; };
+LuTuning g_tuning[32];
+int g_ntuning = 0;
+std::mutex g_tuning_mu;
+}  // namespace
+
+extern "C" int m25_set_lu_tuning(const int *h_n, const int *h_nb2, const int *h_blocks, int count)
+{
+    M25_REQUIRE(count >= 0 && count <= 32 && (count == 0 || (h_n && h_nb2 && h_blocks)),
+                "m25_set_lu_tuning: 0 to 32 entries");
+    LuTuning t[32];
+    for (int i = 0; i < count; ++i) {
+        M25_REQUIRE(h_n[i] >= 1 && h_nb2[i] >= NB && h_nb2[i] <= NB2 && h_nb2[i] % NB == 0 && h_blocks[i] >= 1 &&
+                    h_blocks[i] <= 4096, "m25_set_lu_tuning: n >= 1, nb2 a multiple of 64 up to 256, blocks >= 1");
+        t[i] = LuTuning{h_n[i], h_nb2[i], h_blocks[i]};
+    }
+    std::sort(t, t + count, [](const LuTuning &a, const LuTuning &b) { return a.n < b.n; });
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    std::copy(t, t + count, g_tuning);
+    g_ntuning = count;
+    return M25_OK;
+}
+
+// The parameters a factorisation of size n uses (the tuning table, else the defaults; M25_NB2 and M25_PANEL_BLOCKS
+// in the environment override both).
+extern "C" int m25_get_lu_tuning(int n, int *nb2, int *blocks)
+{
+    int G = sm_count();
+    if (G <= 0) G = 148;
+    int b2 = NB2, gm = std::min(G, 32);
+    {
+        std::lock_guard<std::mutex> lk(g_tuning_mu);
+        if (g_ntuning) {
+            int k = 0;
+            for (int i = 0; i < g_ntuning; ++i)
+                if (g_tuning[i].n <= n) k = i;
+            b2 = g_tuning[k].nb2;
+            gm = std::min(G, g_tuning[k].blocks);
+        }
+    }
+    if (const char *e = getenv("M25_PANEL_BLOCKS")) gm = std::max(1, std::min(G, atoi(e)));
+    if (const char *e = getenv("M25_NB2")) b2 = std::max(NB, std::min(NB2, atoi(e) / NB * NB));
+    if (nb2) *nb2 = b2;
+    if (blocks) *blocks = gm;
+    return M25_OK;
+}
+
 template <typename R>
 static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, size_t work_bytes, cudaStream_t s)
 {
@@ -1383,12 +1398,10 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     // Blocks of the panel: few enough that the cooperative launch finds its SMs quickly while the other stream's
     // update holds the rest (the exchange costs about the same from 37 to 148 blocks), but at least as many as
     // the panel's rows need to fit in shared memory (M25_PANEL_BLOCKS: tuning)
-    int gmax = std::min(G, 32);
-    if (const char *e = getenv("M25_PANEL_BLOCKS")) gmax = std::max(1, std::min(G, atoi(e)));
+    int gmax = 32, nb2 = NB2;                                        // outer panel width and panel blocks: the
+    m25_get_lu_tuning(n, &nb2, &gmax);                               // autotuner's table, else the defaults
     const int rows_cap = (int)((size_t)smem_cap / (sizeof(cpx<R>) * NB));   // a block's rows in shared memory
     const int gcap = std::min(G, PANEL_THREADS);                     // a thread of each block reads a block's record
-    int nb2 = NB2;                                                   // outer panel (M25_NB2: tuning, a multiple of NB)
-    if (const char *e = getenv("M25_NB2")) nb2 = std::max(NB, atoi(e) / NB * NB);
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
     M25_CHECK(cudaFuncSetAttribute(k_zgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdmma_smem()));
     auto laswp = [&](int r0, int nsw, long c0, long c1, cudaStream_t cs) -> int {

@@ -38,8 +38,9 @@ PREDICT_AFTER = 6            # iterations after which a fresh factor's refinemen
 MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
 REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
 REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most
-REUSE_GIVE_UP = (8, 10.0)    # a reused factor's GMRES ends once, after this many steps, its last steps' rate cannot
-                             # bring the residual within this factor of the tolerance by its cap (a fresh LU follows)
+REUSE_GIVE_UP = (12, 100.0)  # a reused factor's GMRES ends once, after this many steps, its last steps' rate cannot
+                             # bring the residual within this factor of the tolerance by its cap (a fresh LU follows;
+                             # measured: from 8 steps with 10x, attempts that converged in 25 were cut off)
 DOUBLE_REACH = float(np.log(1.5))  # |ln f / f0| within which the kept double factor preconditions a double solve
 
 
@@ -153,8 +154,10 @@ class DirectSolver:
         self.tabs = DeviceTables(self.dg, f, single=single, stream=self.stream)
         self.vias = DeviceVias(self.dg, self.tabs, self.stream)
 
-    def impedance(self, f, precision='double'):
-        """Z at f on the device: complex128 (double) or complex64 (mixed)."""
+    def impedance(self, f, precision='double', far=None):
+        """Z at f on the device: complex128 (double) or complex64 (mixed). far: a complex128 N x N tensor whose far
+        part at f is already filled (m25_fill_far_multi with this board's tables at f, the batched sweep): the near
+        field, the via border and the extra blocks are added into it, and it is returned."""
         geo, dg = self.geo, self.dg
         N, Ne = geo.N, geo.Ne
         single = precision == 'mixed'
@@ -165,9 +168,12 @@ class DirectSolver:
         t0 = self._mark()
         qcorr = self._buf('qcorr', (max(1, dg.npairs),), torch.complex128)
         if not single:
-            Z = self._buf('Z', (N, N), torch.complex128)
-            check(lib().m25_fill_far(P(Z), c_long(N), c_int(0), ctypes.byref(dg.mesh), ctypes.byref(tb.tables), None,
-                                     c_double(self.w), s), 'm25_fill_far')
+            if far is not None:
+                Z = far
+            else:
+                Z = self._buf('Z', (N, N), torch.complex128)
+                check(lib().m25_fill_far(P(Z), c_long(N), c_int(0), ctypes.byref(dg.mesh), ctypes.byref(tb.tables),
+                                         None, c_double(self.w), s), 'm25_fill_far')
             check(lib().m25_near(c_int(0), P(Z), c_long(N), c_int(0), None, None, None, P(qcorr), P(dg.stat),
                                  c_int(int(dg.stat_ready)), ctypes.byref(dg.mesh), ctypes.byref(tb.tables),
                                  ctypes.byref(dg.quad), P(dg.nP), P(dg.nQ), c_long(dg.npairs), c_double(self.w), s),
@@ -277,8 +283,10 @@ class DirectSolver:
               'm25_getrs_aux')
         return X
 
-    def solve_direct(self, f, E, block=1024, precision='double'):
-        """Currents for the excitation columns E (N x k, host or device): a complex128 device tensor."""
+    def solve_direct(self, f, E, block=1024, precision='double', far=None):
+        """Currents for the excitation columns E (N x k, host or device): a complex128 device tensor. far: Z with its
+        far part at f already filled (impedance), used in place of a new fill by the mixed path with a resident
+        double Z (the batched sweep)."""
         geo = self.geo
         N = geo.N
         E = torch.as_tensor(np.asarray(E) if not torch.is_tensor(E) else E, dtype=torch.complex128).to('cuda')
@@ -289,8 +297,8 @@ class DirectSolver:
             precision = 'double'                          # fast.py:740: near a failure, double
             if self._hybrid_fits():
                 return self._solve_double_near(f, E)
-        if precision == 'mixed' and self._hybrid_fits():
-            return self._solve_kept(f, E)
+        if precision == 'mixed' and (far is not None or self._hybrid_fits()):
+            return self._solve_kept(f, E, far)
         self.last_path = precision
         single = precision == 'mixed'
         Z = self.impedance(f, precision)
@@ -401,10 +409,10 @@ class DirectSolver:
                 Y[:, c0:c1] = Yc
         return Y
 
-    def _solve_kept(self, f, E):
+    def _solve_kept(self, f, E, far=None):
         """fast.py:996-1084 on the device: returns the currents (equilibration undone)."""
         N = self.geo.N
-        Z = self.impedance(f, 'double')
+        Z = self.impedance(f, 'double', far)
         dsc = self._buf('dsc', (N,), torch.float64)
         check(lib().m25_equilibrate(P(Z), c_long(N), c_long(N), None, P(dsc), None, self.s), 'm25_equilibrate')
         dsc = dsc.clone()

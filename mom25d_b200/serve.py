@@ -36,10 +36,11 @@ GB = 1e9
 
 
 class Request:
-    __slots__ = ('rid', 'board', 'f', 'arrival', 'start', 'done', 'S', 'error', 'slot', 'path', 'iters')
+    __slots__ = ('rid', 'board', 'f', 'arrival', 'start', 'done', 'S', 'error', 'slot', 'path', 'iters', 'far')
 
-    def __init__(self, rid, board, f, arrival=0.0):
+    def __init__(self, rid, board, f, arrival=0.0, far=None):
         self.rid, self.board, self.f, self.arrival = rid, board, float(f), float(arrival)
+        self.far = far                  # Z with the far part at f already filled (the batched sweep), or None
         self.start = self.done = None
         self.S = self.error = self.slot = self.path = None
         self.iters = []
@@ -128,16 +129,23 @@ class Server:
             with torch.cuda.stream(self._streams[slot]):
                 ds = DirectSolver(self._geometry(key), stream=self._streams[slot], tf32=umma_available())
                 ds.reuse = False                       # results independent of the request order
+                ds.hybrid = True                       # the admission has reserved the double Z's room
                 self._solvers[(slot, key)] = ds
         return self._solvers[(slot, key)], self._streams[slot]
 
-    def _solve_gpu(self, slot, key, f):
+    def _solve_gpu(self, slot, key, f, far=None):
         import torch
+        from .operator import SolveFailed
         ds, stream = self._solver(slot, key)
         geo = self._geometry(key)
         with torch.cuda.stream(stream):
             try:
-                X = ds.solve_direct(f, geo.excitation(), precision=self.precision)
+                if far is not None:
+                    stream.wait_stream(torch.cuda.default_stream())    # (filled on the default stream)
+                try:
+                    X = ds.solve_direct(f, geo.excitation(), precision=self.precision, far=far)
+                except SolveFailed:                     # (sim.py's rule: the frequency again in double precision)
+                    X = ds.solve_direct(f, geo.excitation(), precision='double')
                 S = geo.sparams_from_currents(X.cpu().numpy(), f)
                 stream.synchronize()
                 del X
@@ -181,7 +189,9 @@ class Server:
                     return
                 r.start = clock() - t0
                 try:
-                    r.S, info = self._solve(slot, r.board, r.f)
+                    r.S, info = self._solve(slot, r.board, r.f) if r.far is None else \
+                        self._solve(slot, r.board, r.f, far=r.far)
+                    r.far = None
                     r.path, r.iters = info.get('path'), info.get('iters', [])
                 except Exception as e:                   # reported on the request; the loop keeps serving
                     r.error = f"{type(e).__name__}: {e}"
@@ -269,6 +279,7 @@ class Server:
     def report(reqs, wall):
         lat = np.array([r.latency for r in reqs if r.error is None])
         return dict(requests=len(reqs), errors=sum(r.error is not None for r in reqs),
+                    error_messages=sorted({r.error for r in reqs if r.error is not None})[:3],
                     solves_per_s=round(len(lat) / wall, 3) if wall > 0 else None,
                     p50_ms=round(1000 * float(np.percentile(lat, 50)), 1) if len(lat) else None,
                     p99_ms=round(1000 * float(np.percentile(lat, 99)), 1) if len(lat) else None)

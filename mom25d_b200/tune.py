@@ -1,6 +1,7 @@
 """
-mom25d_b200.tune - timings of the hot path's kernels on this GPU, and the choice of their tile parameters.
+mom25d_b200.tune - the autotuner of the LU's tile parameters, and timings of the hot path's kernels on this GPU.
 
+    python -m mom25d_b200.tune --autotune [--sizes 2000 5000 10000 20000 40000] [--write]
     python -m mom25d_b200.tune --lu 8192 [--single] [--tf32] [--reps 3]     # the LU alone, CUDA events
     python -m mom25d_b200.tune --update 4096 4096 256                        # the tensor-core trailing update
     python -m mom25d_b200.tune --solve 18788 [--single]                      # the triangular solves, 8 columns
@@ -8,7 +9,16 @@ mom25d_b200.tune - timings of the hot path's kernels on this GPU, and the choice
 
 Times are CUDA-event measurements on the launching stream after a warm-up, the matrix a random complex one with a
 dominant diagonal (pivots away from it as well).
+
+The autotuner times the complex64 LU with tensor-core updates (the mixed path's factorisation) at each size over
+a grid of its two host-side parameters: the outer panel width (the depth of the tensor-core trailing updates,
+128 / 192 / 256 columns) and the number of CTAs of the cooperative panel kernel (16 to 64). The fastest pair per
+size goes into TUNING_FILE ({"device", "sms", "entries": [{"n", "nb2", "blocks", "ms"}]}), which the library
+reads at load (_lib.apply_tuning -> m25_set_lu_tuning): a factorisation takes the entry with the largest n at or
+below its own. The tensor-core kernel's stage count is a compile-time choice (two stages, two CTAs an SM) and is
+not searched.
 """
+import os
 import argparse
 import ctypes
 import json
@@ -28,6 +38,49 @@ def random_matrix(n, dtype, seed=0):
                       torch.randn(n, n, generator=g, device='cuda', dtype=rdt))
     Z.diagonal().add_(4 * n ** 0.5)
     return Z
+
+
+TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'tuning_b200.json')
+NB2_GRID = (128, 192, 256)
+BLOCK_GRID = (16, 24, 32, 48, 64)
+
+
+def set_table(entries):
+    """The LU's tuning table in the library: [(n, nb2, blocks)]."""
+    arr = lambda i: (ctypes.c_int * max(1, len(entries)))(*[e[i] for e in entries])
+    check(lib().m25_set_lu_tuning(arr(0), arr(1), arr(2), len(entries)), 'm25_set_lu_tuning')
+
+
+def autotune(sizes, reps=2, log=print):
+    """The fastest (nb2, blocks) per size: [{n, nb2, blocks, ms, grid: {"nb2/blocks": ms}}]."""
+    out = []
+    for n in sizes:
+        grid = [(b2, bl) for b2 in NB2_GRID for bl in BLOCK_GRID]
+        if n > 30000:                                     # (the largest size: a coarser grid, each LU is seconds)
+            grid = [(b2, bl) for b2 in (192, 256) for bl in (32, 64)]
+        times = {}
+        for b2, bl in grid:
+            set_table([(1, b2, bl)])
+            times[f"{b2}/{bl}"] = time_lu(n, single=True, tf32=True, reps=reps)['ms']
+        best = min(times, key=times.get)
+        b2, bl = map(int, best.split('/'))
+        out.append(dict(n=int(n), nb2=b2, blocks=bl, ms=round(times[best], 2), grid={k: round(v, 2) for k, v in
+                                                                                     times.items()}))
+        if log:
+            log(f"n={n}: nb2 {b2}, panel blocks {bl}: {times[best]:.1f} ms (default 256/32: "
+                f"{times.get('256/32', float('nan')):.1f} ms)")
+    set_table([(e['n'], e['nb2'], e['blocks']) for e in out])
+    return out
+
+
+def write_tuning(entries, path=TUNING_FILE):
+    import torch
+    props = torch.cuda.get_device_properties(0)
+    doc = dict(device=props.name, sms=props.multi_processor_count,
+               entries=[{k: e[k] for k in ('n', 'nb2', 'blocks', 'ms')} for e in entries])
+    with open(path, 'w') as fh:
+        json.dump(doc, fh, indent=1)
+    return path
 
 
 def time_lu(n, single=False, tf32=False, reps=3):
@@ -136,8 +189,16 @@ def main():
     ap.add_argument('--single', action='store_true')
     ap.add_argument('--tf32', action='store_true')
     ap.add_argument('--reps', type=int, default=3)
+    ap.add_argument('--autotune', action='store_true')
+    ap.add_argument('--sizes', type=int, nargs='+', default=[2000, 5000, 10000, 20000, 40000])
+    ap.add_argument('--write', action='store_true', help='write the autotuner\'s table to ' + TUNING_FILE)
     a = ap.parse_args()
     _lib.require_cuda()
+    if a.autotune:
+        entries = autotune(a.sizes, reps=max(1, min(a.reps, 2)))
+        print(json.dumps(entries))
+        if a.write:
+            print('wrote', write_tuning(entries))
     if a.lu:
         print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
     if a.update:

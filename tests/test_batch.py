@@ -26,7 +26,7 @@ def test_sweep_runs_every_frequency_concurrently_in_order():
     freqs = np.linspace(1e9, 6e9, 12)
     srv = Server({'b': None}, slots=4, budget_bytes=100 * GB, solve=solve, sizes={'b': 8000}, ports={'b': 2},
                  resident=lambda slot, key: 0.0, evict=lambda slot, key: None)
-    S, wall, reqs = batched_sweep(srv, 'b', freqs)
+    S, wall, reqs = batched_sweep(srv, 'b', freqs, multi=False)
     assert [s[0, 0].real for s in S] == list(freqs)          # frequency order, whatever the completion order
     assert seen['max'] == 4 and all(r.path == 'fresh' for r in reqs)
     assert wall < 12 * 0.02                                   # overlapped, not one after another
