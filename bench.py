@@ -245,8 +245,9 @@ def run_gpu(args, rank, world):
         step_path.append(ds.last_path)
         kept_X.append(X)                    # compared with the FP64 solve of the same frequency below
         if args.verbose:
+            rh = getattr(ds, 'res_hist', [])
             print(f"step {i}: {mine[i % len(mine)] / 1e9:.4g} GHz {ds.last_path:22s} {iters[-1]:3d} iterations "
-                  f"{ms:8.1f} ms", file=sys.stderr)
+                  f"{ms:8.1f} ms  residual by step: " + ' '.join(f"{x:.0e}" for x in rh[1::3]), file=sys.stderr)
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()

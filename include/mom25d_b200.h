@@ -248,13 +248,14 @@ size_t m25_getrf_workspace(int n, int single);
  * only): trailing updates on the tensor cores as 3xTF32 products. */
 int m25_getrf(void *d_A, long lda, int n, int *d_ipiv, int single, int tf32, void *d_work, size_t work_bytes,
               void *stream);
-/* The LU's tile parameters by matrix size (no counterpart in the reference: LAPACK picks its own blocking): up to
- * 32 entries (n, outer panel width nb2 = 64..256 in steps of 64, cooperative panel blocks), as the autotuner
- * (mom25d_b200/tune.py) finds them on this GPU; a factorisation of size n takes the entry with the largest n at or
- * below its own. count 0 restores the defaults (256, min(SMs, 32)). The environment variables M25_NB2 and
- * M25_PANEL_BLOCKS override both. m25_get_lu_tuning: what a factorisation of size n uses. */
-int m25_set_lu_tuning(const int *h_n, const int *h_nb2, const int *h_blocks, int count);
-int m25_get_lu_tuning(int n, int *nb2, int *blocks);
+/* The LU's tile parameters by matrix size (no counterpart in the reference: LAPACK picks its own blocking): a
+ * table for complex64 (single = 1) and one for complex128 factorisations, up to 32 entries each (n, outer panel
+ * width nb2 = 64..256 in steps of 64, cooperative panel blocks), as the autotuner (mom25d_b200/tune.py) finds them
+ * on this GPU; a factorisation of size n takes the entry nearest to n in log n. count 0 restores the defaults
+ * (256, min(SMs, 32)). The environment variables M25_NB2 and M25_PANEL_BLOCKS override both.
+ * m25_get_lu_tuning: what a factorisation of size n uses. */
+int m25_set_lu_tuning(int single, const int *h_n, const int *h_nb2, const int *h_blocks, int count);
+int m25_get_lu_tuning(int n, int single, int *nb2, int *blocks);
 /* Solves Z X = B with the factor of Z^T (lu_solve(..., trans=1)); B (row-major n x nrhs, complex in the factor's
  * precision) overwritten by X. */
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);

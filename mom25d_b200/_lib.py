@@ -74,9 +74,12 @@ def apply_tuning(L, path=None):
             return False
     except Exception:
         pass
-    ent = doc.get('entries', [])
-    arr = lambda k: (ctypes.c_int * max(1, len(ent)))(*[int(e[k]) for e in ent])
-    return L.m25_set_lu_tuning(arr('n'), arr('nb2'), arr('blocks'), len(ent)) == 0
+    ok = True
+    for single, key in ((1, 'complex64'), (0, 'complex128')):
+        ent = doc.get(key, [])
+        arr = lambda k: (ctypes.c_int * max(1, len(ent)))(*[int(e[k]) for e in ent])
+        ok = L.m25_set_lu_tuning(single, arr('n'), arr('nb2'), arr('blocks'), len(ent)) == 0 and ok
+    return ok
 
 
 def check(rc, what=''):

@@ -1276,7 +1276,7 @@ extern "C" size_t m25_getrf_workspace(int n, int single)
 // created on the thread's first factorisation there (calls from different threads, e.g. concurrent requests on
 // their own streams, do not share them; calls from one thread are ordered by it).
 namespace {
-struct LuStreams { cudaStream_t hi = nullptr, lo = nullptr; cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; };
+struct LuStreams { cudaStream_t hi = nullptr, lo = nullptr; cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr}; };
 thread_local LuStreams g_lu[64];
 
 int lu_streams(LuStreams *out)
@@ -1298,16 +1298,16 @@ int lu_streams(LuStreams *out)
 }  // namespace
 
 // ---- the LU's tile parameters by matrix size (set by the autotuner, mom25d_b200.tune) --------------------------------
-// Entries (n, outer panel width, panel blocks), sorted by n; a factorisation of size n takes the entry with the
-// largest n at or below its own (the first entry below all of them). Without entries: NB2 and min(SMs, 32).
+// Two tables, complex64 and complex128, of entries (n, outer panel width, panel blocks); a factorisation of size n
+// takes the entry nearest to n in log n. Without entries: NB2 and min(SMs, 32).
 namespace {
 struct LuTuning { int n, nb2, blocks; };
-LuTuning g_tuning[32];
-int g_ntuning = 0;
+LuTuning g_tuning[2][32];
+int g_ntuning[2] = {0, 0};
 std::mutex g_tuning_mu;
 }  // namespace
 
-extern "C" int m25_set_lu_tuning(const int *h_n, const int *h_nb2, const int *h_blocks, int count)
+extern "C" int m25_set_lu_tuning(int single, const int *h_n, const int *h_nb2, const int *h_blocks, int count)
 {
     M25_REQUIRE(count >= 0 && count <= 32 && (count == 0 || (h_n && h_nb2 && h_blocks)),
                 "m25_set_lu_tuning: 0 to 32 entries");
@@ -1319,26 +1319,31 @@ extern "C" int m25_set_lu_tuning(const int *h_n, const int *h_nb2, const int *h_
     }
     std::sort(t, t + count, [](const LuTuning &a, const LuTuning &b) { return a.n < b.n; });
     std::lock_guard<std::mutex> lk(g_tuning_mu);
-    std::copy(t, t + count, g_tuning);
-    g_ntuning = count;
+    const int w = single ? 1 : 0;
+    std::copy(t, t + count, g_tuning[w]);
+    g_ntuning[w] = count;
     return M25_OK;
 }
 
-// The parameters a factorisation of size n uses (the tuning table, else the defaults; M25_NB2 and M25_PANEL_BLOCKS
-// in the environment override both).
-extern "C" int m25_get_lu_tuning(int n, int *nb2, int *blocks)
+// The parameters a factorisation of size n (complex64 when single) uses: the table's entry nearest in log n, else
+// the defaults; M25_NB2 and M25_PANEL_BLOCKS in the environment override both.
+extern "C" int m25_get_lu_tuning(int n, int single, int *nb2, int *blocks)
 {
     int G = sm_count();
     if (G <= 0) G = 148;
     int b2 = NB2, gm = std::min(G, 32);
     {
         std::lock_guard<std::mutex> lk(g_tuning_mu);
-        if (g_ntuning) {
+        const int w = single ? 1 : 0;
+        if (g_ntuning[w]) {
             int k = 0;
-            for (int i = 0; i < g_ntuning; ++i)
-                if (g_tuning[i].n <= n) k = i;
-            b2 = g_tuning[k].nb2;
-            gm = std::min(G, g_tuning[k].blocks);
+            double best = 1e300;
+            for (int i = 0; i < g_ntuning[w]; ++i) {
+                const double d = fabs(log((double)g_tuning[w][i].n / (double)std::max(1, n)));
+                if (d < best) { best = d; k = i; }
+            }
+            b2 = g_tuning[w][k].nb2;
+            gm = std::min(G, g_tuning[w][k].blocks);
         }
     }
     if (const char *e = getenv("M25_PANEL_BLOCKS")) gm = std::max(1, std::min(G, atoi(e)));
@@ -1380,7 +1385,7 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     if (rc) return rc;
     const char *la = getenv("M25_LOOKAHEAD");                       // 0: one stream (the same results, in order)
     const cudaStream_t H = st.hi, Lo = (la && atoi(la) == 0) ? st.hi : st.lo;
-    cudaEvent_t ev_start = st.ev[0], ev_p = st.ev[1], ev_u = st.ev[2], ev_end = st.ev[3];
+    cudaEvent_t ev_start = st.ev[0], ev_panel = st.ev[1], ev_next = st.ev[2], ev_lo = st.ev[3], ev_end = st.ev[4];
     M25_CHECK(cudaEventRecord(ev_start, s));                        // the caller's work first
     M25_CHECK(cudaStreamWaitEvent(H, ev_start, 0));
     M25_CHECK(cudaStreamWaitEvent(Lo, ev_start, 0));
@@ -1399,7 +1404,7 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     // update holds the rest (the exchange costs about the same from 37 to 148 blocks), but at least as many as
     // the panel's rows need to fit in shared memory (M25_PANEL_BLOCKS: tuning)
     int gmax = 32, nb2 = NB2;                                        // outer panel width and panel blocks: the
-    m25_get_lu_tuning(n, &nb2, &gmax);                               // autotuner's table, else the defaults
+    m25_get_lu_tuning(n, sizeof(R) == 4, &nb2, &gmax);               // autotuner's table, else the defaults
     const int rows_cap = (int)((size_t)smem_cap / (sizeof(cpx<R>) * NB));   // a block's rows in shared memory
     const int gcap = std::min(G, PANEL_THREADS);                     // a thread of each block reads a block's record
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
@@ -1446,13 +1451,21 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
         return M25_OK;
     };
     // Two levels: outer panels of nb2 columns, each factored as panels of NB (pivoting, interchanges, TRSM and
-    // updates restricted to the outer panel); then the outer panel's interchanges, TRSM and the trailing update of
-    // depth nb2. Look-ahead: the update of the next outer panel's columns runs on the high-priority stream H, the
-    // update of all the columns after it on the low-priority stream Lo, while H factors the next outer panel
-    // (disjoint columns); H waits for Lo before it touches those columns (interchanges, TRSM) again.
-    bool lo_pending = false;
+    // updates restricted to the outer panel). Then, for outer block k of columns [K0, KE), the next block's columns
+    // [KE, KE2) and the rest [KE2, n):
+    //   H (high priority, the critical path): the next block's interchanges, U12 and update by block k, then the
+    //     next block's panels. Before touching those columns it waits only for the part of the previous block's
+    //     low-priority update that covers them (ev_next), which that update does first;
+    //   Lo (low priority): as soon as block k's panels are done (ev_panel), block k's interchanges on the columns
+    //     left of it and on [KE2, n), U12 of [KE2, n), then the update of [KE2, n): first the columns of block
+    //     k + 2 ([KE2, KE3): ev_next, which H waits for at block k + 1), then the rest.
+    // Regions: H works on columns >= KE only; Lo on columns < K0 (interchanges) and >= KE2; both read block k's
+    // L (rows >= KE of columns [K0, KE)), which nothing writes until block k + 1's left interchanges, issued on Lo
+    // after this update. Lo's work for a block follows its work for the previous block (stream order).
+    bool next_pending = false;
     for (int K0 = 0; K0 < n; K0 += nb2) {
         const int JB = std::min(nb2, n - K0), KE = K0 + JB;
+        const int KE2 = std::min(n, KE + nb2), KE3 = std::min(n, KE2 + nb2);
         for (int k0 = K0; k0 < KE; k0 += NB) {
             const int jb = std::min(NB, KE - k0);
             int Gp = std::min(gmax, std::max(1, (n - k0 + 31) / 32));
@@ -1477,29 +1490,35 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             // board no longer converged; the FP32 inner update costs 5 ms of 236 at N = 18,788)
             if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, false, H))) return rc;
         }
-        if (lo_pending) {                                                   // the previous block's update of [KE, n)
-            M25_CHECK(cudaStreamWaitEvent(H, ev_u, 0));                     // reads L of the earlier columns: their
-            lo_pending = false;                                             // interchanges wait for it
-        }
-        if ((rc = laswp(K0, JB, 0, K0, H))) return rc;                     // the outer panel's interchanges, left
-        if (KE < n) {
-            if ((rc = laswp(K0, JB, KE, n, H))) return rc;                 // the outer panel's interchanges, right
+        M25_CHECK(cudaEventRecord(ev_panel, H));                          // block k's L and pivots are final
+        if (KE < n) {                                                       // H: the next block's columns
+            if (next_pending) M25_CHECK(cudaStreamWaitEvent(H, ev_next, 0));
+            if ((rc = laswp(K0, JB, KE, KE2, H))) return rc;
             for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
                 const int jb = std::min(NB, KE - k0);
-                if ((rc = trsm(k0, jb, KE, n, H))) return rc;
-                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, n - KE, k0, jb, true, H))) return rc;
+                if ((rc = trsm(k0, jb, KE, KE2, H))) return rc;
+                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, KE2 - KE, k0, jb, true, H))) return rc;
             }
-            const int KE2 = std::min(n, KE + nb2);                          // the next outer panel's columns
             if ((rc = gemm(KE, n - KE, KE, KE2 - KE, K0, JB, true, H))) return rc;
-            if (KE2 < n) {                                                  // the rest, beside the next panels
-                M25_CHECK(cudaEventRecord(ev_p, H));
-                M25_CHECK(cudaStreamWaitEvent(Lo, ev_p, 0));
-                if ((rc = gemm(KE, n - KE, KE2, n - KE2, K0, JB, true, Lo))) return rc;
-                M25_CHECK(cudaEventRecord(ev_u, Lo));
-                lo_pending = true;
+        }
+        M25_CHECK(cudaStreamWaitEvent(Lo, ev_panel, 0));                    // Lo: the left and the far columns
+        if ((rc = laswp(K0, JB, 0, K0, Lo))) return rc;
+        next_pending = false;
+        if (KE2 < n) {
+            if ((rc = laswp(K0, JB, KE2, n, Lo))) return rc;
+            for (int k0 = K0; k0 < KE; k0 += NB) {
+                const int jb = std::min(NB, KE - k0);
+                if ((rc = trsm(k0, jb, KE2, n, Lo))) return rc;
+                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE2, n - KE2, k0, jb, true, Lo))) return rc;
             }
+            if ((rc = gemm(KE, n - KE, KE2, KE3 - KE2, K0, JB, true, Lo))) return rc;   // block k + 2's columns
+            M25_CHECK(cudaEventRecord(ev_next, Lo));
+            next_pending = true;
+            if ((rc = gemm(KE, n - KE, KE3, n - KE3, K0, JB, true, Lo))) return rc;    // the rest
         }
     }
+    M25_CHECK(cudaEventRecord(ev_lo, Lo));                           // the last left interchanges, then the end
+    M25_CHECK(cudaStreamWaitEvent(H, ev_lo, 0));
     M25_CHECK(cudaEventRecord(ev_end, H));                           // the caller's stream waits for both
     M25_CHECK(cudaStreamWaitEvent(s, ev_end, 0));
     return M25_OK;

@@ -598,6 +598,8 @@ class DirectSolver:
                 rate = (res[act] / bn[act]) ** (1.0 / (j + 1))
                 if (res[act] * rate ** (restart - j - 1) > 10 * rtol * bn[act]).any():
                     break
+        # the largest relative residual estimate after each step (diagnostics: the bench's verbose log)
+        self.res_hist = [float((h / bn).max()) for h in hist]
         # y per column from its own steps, Y = sum_j Z_j y_j
         m = int(steps.max())
         coef = np.zeros((m, k), complex)

@@ -10,13 +10,15 @@ mom25d_b200.tune - the autotuner of the LU's tile parameters, and timings of the
 Times are CUDA-event measurements on the launching stream after a warm-up, the matrix a random complex one with a
 dominant diagonal (pivots away from it as well).
 
-The autotuner times the complex64 LU with tensor-core updates (the mixed path's factorisation) at each size over
-a grid of its two host-side parameters: the outer panel width (the depth of the tensor-core trailing updates,
-128 / 192 / 256 columns) and the number of CTAs of the cooperative panel kernel (16 to 64). The fastest pair per
-size goes into TUNING_FILE ({"device", "sms", "entries": [{"n", "nb2", "blocks", "ms"}]}), which the library
-reads at load (_lib.apply_tuning -> m25_set_lu_tuning): a factorisation takes the entry with the largest n at or
-below its own. The tensor-core kernel's stage count is a compile-time choice (two stages, two CTAs an SM) and is
-not searched.
+The autotuner times the LU at each size over its host-side parameters and keeps the fastest: for the complex64
+LU with tensor-core updates (the mixed path's factorisation) the number of CTAs of the cooperative panel kernel
+(16 to 64), its outer panel width kept at 256 columns - a narrower one leaves more of the factor's updates to
+3xTF32 instead of FP32 and costs the factor its use as a preconditioner at the low-frequency end (measured on the
+routed board: with 128, the fresh factor at 0.67 GHz no longer converged); for the complex128 LU (the drop-in)
+both the outer panel width (128 / 192 / 256) and the panel CTAs. The winners per size go into TUNING_FILE
+({"device", "sms", "complex64": [{"n", "nb2", "blocks", "ms"}], "complex128": [...]}), which the library reads at
+load (_lib.apply_tuning -> m25_set_lu_tuning): a factorisation takes the entry nearest its size. The tensor-core
+kernel's stage count is a compile-time choice (two stages, two CTAs an SM) and is not searched.
 """
 import os
 import argparse
@@ -41,43 +43,44 @@ def random_matrix(n, dtype, seed=0):
 
 
 TUNING_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'tuning_b200.json')
-NB2_GRID = (128, 192, 256)
-BLOCK_GRID = (16, 24, 32, 48, 64)
+GRIDS = {True: [(256, bl) for bl in (16, 24, 32, 48, 64)],
+         False: [(b2, bl) for b2 in (128, 192, 256) for bl in (16, 32, 48)]}
 
 
-def set_table(entries):
-    """The LU's tuning table in the library: [(n, nb2, blocks)]."""
+def set_table(entries, single=True):
+    """The LU's tuning table in the library: [(n, nb2, blocks)] for complex64 (single) or complex128."""
     arr = lambda i: (ctypes.c_int * max(1, len(entries)))(*[e[i] for e in entries])
-    check(lib().m25_set_lu_tuning(arr(0), arr(1), arr(2), len(entries)), 'm25_set_lu_tuning')
+    check(lib().m25_set_lu_tuning(int(single), arr(0), arr(1), arr(2), len(entries)), 'm25_set_lu_tuning')
 
 
-def autotune(sizes, reps=2, log=print):
-    """The fastest (nb2, blocks) per size: [{n, nb2, blocks, ms, grid: {"nb2/blocks": ms}}]."""
+def autotune(sizes, single=True, reps=2, log=print):
+    """The fastest (nb2, blocks) per size for the complex64 (tensor-core) or complex128 LU:
+    [{n, nb2, blocks, ms, grid: {"nb2/blocks": ms}}]."""
     out = []
     for n in sizes:
-        grid = [(b2, bl) for b2 in NB2_GRID for bl in BLOCK_GRID]
+        grid = GRIDS[single]
         if n > 30000:                                     # (the largest size: a coarser grid, each LU is seconds)
-            grid = [(b2, bl) for b2 in (192, 256) for bl in (32, 64)]
+            grid = [g for g in grid if g[1] in (32, 48)][:4]
         times = {}
         for b2, bl in grid:
-            set_table([(1, b2, bl)])
-            times[f"{b2}/{bl}"] = time_lu(n, single=True, tf32=True, reps=reps)['ms']
+            set_table([(1, b2, bl)], single)
+            times[f"{b2}/{bl}"] = time_lu(n, single=single, tf32=single, reps=reps)['ms']
         best = min(times, key=times.get)
         b2, bl = map(int, best.split('/'))
         out.append(dict(n=int(n), nb2=b2, blocks=bl, ms=round(times[best], 2), grid={k: round(v, 2) for k, v in
                                                                                      times.items()}))
         if log:
-            log(f"n={n}: nb2 {b2}, panel blocks {bl}: {times[best]:.1f} ms (default 256/32: "
-                f"{times.get('256/32', float('nan')):.1f} ms)")
-    set_table([(e['n'], e['nb2'], e['blocks']) for e in out])
+            log(f"{'complex64' if single else 'complex128'} n={n}: nb2 {b2}, panel blocks {bl}: {times[best]:.1f} ms "
+                f"(default 256/32: {times.get('256/32', float('nan')):.1f} ms)")
+    set_table([(e['n'], e['nb2'], e['blocks']) for e in out], single)
     return out
 
 
-def write_tuning(entries, path=TUNING_FILE):
+def write_tuning(c64, c128, path=TUNING_FILE):
     import torch
     props = torch.cuda.get_device_properties(0)
-    doc = dict(device=props.name, sms=props.multi_processor_count,
-               entries=[{k: e[k] for k in ('n', 'nb2', 'blocks', 'ms')} for e in entries])
+    keep = lambda es: [{k: e[k] for k in ('n', 'nb2', 'blocks', 'ms')} for e in es]
+    doc = dict(device=props.name, sms=props.multi_processor_count, complex64=keep(c64), complex128=keep(c128))
     with open(path, 'w') as fh:
         json.dump(doc, fh, indent=1)
     return path
@@ -195,10 +198,11 @@ def main():
     a = ap.parse_args()
     _lib.require_cuda()
     if a.autotune:
-        entries = autotune(a.sizes, reps=max(1, min(a.reps, 2)))
-        print(json.dumps(entries))
+        c64 = autotune(a.sizes, single=True, reps=max(1, min(a.reps, 2)))
+        c128 = autotune([n for n in a.sizes if n <= 20000], single=False, reps=1)
+        print(json.dumps(dict(complex64=c64, complex128=c128)))
         if a.write:
-            print('wrote', write_tuning(entries))
+            print('wrote', write_tuning(c64, c128))
     if a.lu:
         print(json.dumps(time_lu(a.lu, a.single, a.tf32, a.reps)))
     if a.update:

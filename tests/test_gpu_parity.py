@@ -214,8 +214,7 @@ def test_dense_double_product(k):
     assert np.abs(Yd.cpu().numpy() - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize('single', [0, 1])
-@pytest.mark.parametrize('n', [300, 1000])
+@pytest.mark.parametrize('single,n', [(0, 300), (1, 300), (0, 1000), (1, 1000), (0, 3001)])
 def test_lu_matches_lapack(single, n):
     """The LU against LAPACK (SciPy's lu_factor of Z^T): the same pivots, the factor to round-off, the solves
     (the reference's own LU test, test_gpu.py:210-235: N = 300, + 4 sqrt(N) I, rows 0 and 7 interchanged)."""
@@ -256,10 +255,11 @@ def test_complex_bessel_matches_the_reference(golden):
         assert np.abs(out.cpu().numpy() - ref).max() <= 1e-13 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize('n', [700, 2000])
+@pytest.mark.parametrize('n', [700, 2000, 4100])
 def test_lu_with_tensor_core_updates(n):
     """The complex64 LU with its trailing updates on the tensor cores (3xTF32): a factor as good as the FP32 one
-    (backward error at single-precision level) and solves that match."""
+    (backward error at single-precision level) and solves that match. 4100: 17 outer blocks, the last ragged, so
+    every part of the two-stream schedule runs (the look-ahead columns, the far columns' first slice and rest)."""
     from mom25d_b200 import _lib
     rng = np.random.default_rng(5)
     Z = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
