@@ -56,10 +56,51 @@ def fill_far_sweep(geo, dg, freqs, stream=None):
     return Zs, tabs
 
 
-def batched_sweep(server, key, freqs, multi=True):
+class _ChunkFill:
+    """The far part of a sweep's Z filled chunk by chunk on a stream and host thread of its own, one launch a chunk
+    (fill_far_sweep), while the serving loop solves the chunks already filled: request i's far() waits for its
+    chunk, then hands over its Z (and lets go of it)."""
+
+    def __init__(self, geo, dg, freqs, chunk):
+        import threading
+        import torch
+        self.freqs, self.chunk = [float(f) for f in freqs], chunk
+        self.ready = [threading.Event() for _ in range(0, len(freqs), chunk)]
+        self.Z, self.error = {}, None
+        self.stream = torch.cuda.Stream()
+        self.thread = threading.Thread(target=self._run, args=(geo, dg), daemon=True)
+        self.thread.start()
+
+    def _run(self, geo, dg):
+        import torch
+        try:
+            with torch.cuda.stream(self.stream):
+                for c, c0 in enumerate(range(0, len(self.freqs), self.chunk)):
+                    part = self.freqs[c0:c0 + self.chunk]
+                    Zs, tabs = fill_far_sweep(geo, dg, part, stream=self.stream)
+                    for i, Z in enumerate(Zs):
+                        self.Z[c0 + i] = Z
+                    del Zs, tabs
+                    self.ready[c].set()
+        except Exception as e:                     # the requests of the chunks not filled report it
+            self.error = e
+            for ev in self.ready:
+                ev.set()
+
+    def far(self, i):
+        def get():
+            self.ready[i // self.chunk].wait()
+            if self.error is not None:
+                raise RuntimeError(f"batched sweep: the far fill failed: {self.error}")
+            return self.Z.pop(i)
+        return get
+
+
+def batched_sweep(server, key, freqs, multi=True, chunk=None):
     """All frequencies through the server at once: (S list in frequency order, wall seconds, requests). multi: the
-    far part of every frequency's Z filled first by one launch (in chunks of what fits), the requests carrying
-    their Z; else each request fills its own."""
+    far part of every frequency's Z filled by one launch a chunk (default: a quarter of the sweep, as memory
+    allows) on a stream of its own, overlapping the solves of the chunks before it, the requests carrying their Z;
+    else each request fills its own."""
     t = time.perf_counter()
     if not multi:
         reqs = sweep_requests(key, freqs)
@@ -75,16 +116,12 @@ def batched_sweep(server, key, freqs, multi=True):
         free, _ = torch.cuda.mem_get_info()
         per = 16.0 * geo.N * geo.N
         room = 0.8 * free - server.slots * (server.footprint(key) + 2e9)
-        chunk = max(1, min(len(freqs), int(room // per)))
-        reqs = []
-        for c0 in range(0, len(freqs), chunk):
-            part = [float(f) for f in freqs[c0:c0 + chunk]]
-            Zs, tabs = fill_far_sweep(geo, dg, part)
-            rq = [Request(c0 + i, key, f, 0.0, far=Z) for i, (f, Z) in enumerate(zip(part, Zs))]
-            del Zs
-            server.run(rq)
-            reqs += rq
-            del rq, tabs
+        fits = max(1, int(room // per) // 2)                 # (two chunks in memory at once)
+        chunk = max(1, min(chunk or -(-len(freqs) // 4), fits))
+        filler = _ChunkFill(geo, dg, freqs, chunk)
+        reqs = [Request(i, key, f, 0.0, far=filler.far(i)) for i, f in enumerate(freqs)]
+        server.run(reqs)
+        filler.thread.join()
     wall = time.perf_counter() - t
     bad = [r for r in reqs if r.error is not None]
     if bad:

@@ -21,21 +21,26 @@ int *m25_dev_err_word();
 
 namespace {
 
-// tile of C' (rows x cols), K floats per stage (16 floats = 64 B rows: 64B swizzle). Two stages a CTA, so that two
-// CTAs fit an SM (2 x 97 KB of shared memory, 2 x 256 tensor-memory columns): one's epilogue (C read, updated and
-// written back) runs while the other multiplies, which one CTA with four stages could not do (3.92 -> 3.38 ms for
-// an 18,000 x 18,000 x 256 complex update)
-constexpr int BM = 128, BN = 256, BKF = 16;
+// tile of C' (rows x cols), BKF floats of K per stage. Two stages of 16 floats (64-byte rows, 64B swizzle): 48 KB a
+// stage, 97 KB a CTA, so two CTAs fit an SM (2 x 256 tensor-memory columns) and one's epilogue (C read, updated and
+// written back) runs while the other multiplies, which one CTA with four stages could not do (3.92 -> 3.38 ms for an
+// 18,000 x 18,000 x 256 complex update). Measured and not kept: four stages of 8 floats (32-byte rows, the same
+// 97 KB): 4.23 ms, the tensor pipe 40% busy against 64% (smaller TMA boxes, a commit every three MMAs).
+#ifndef M25_UMMA_BKF
+#define M25_UMMA_BKF 16
+#endif
 #ifndef M25_UMMA_STAGES
 #define M25_UMMA_STAGES 2
 #endif
+constexpr int BM = 128, BN = 256, BKF = M25_UMMA_BKF;
 constexpr int STAGES = M25_UMMA_STAGES;
-constexpr int CTAS_PER_SM = STAGES <= 2 ? 2 : 1;           // two CTAs an SM when their stages fit twice
 constexpr int SWZ_BYTES = BKF * 4;                   // the swizzle span: one K row of a stage
-static_assert(SWZ_BYTES == 64 || SWZ_BYTES == 128, "64B or 128B swizzle");
+static_assert(SWZ_BYTES == 32 || SWZ_BYTES == 64 || SWZ_BYTES == 128, "32B, 64B or 128B swizzle");
 constexpr int A_BYTES = BM * BKF * 4, B_BYTES = BN * BKF * 4;
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;          // hi and lo of A' and B'
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // + alignment slack + barriers
+constexpr int CTAS_PER_SM = 2 * SMEM_BYTES <= 226 * 1024 ? 2 : 1;   // two CTAs an SM when their stages fit twice
+static_assert(STAGE_BYTES % 1024 == 0, "stages on 1024-byte boundaries (swizzle atoms)");
 constexpr unsigned TMEM_COLS = 256;
 constexpr long WAIT_LIMIT = 1L << 24;
 
@@ -74,7 +79,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
 }
 
 // shared-memory matrix descriptor: K-major, swizzled rows of SWZ_BYTES, 8-row groups 8 x SWZ_BYTES apart
-// (tcgen05 layout, version 1; layout type 2 = 128B swizzle, 4 = 64B swizzle)
+// (tcgen05 layout, version 1; layout type 2 = 128B swizzle, 4 = 64B swizzle, 6 = 32B swizzle)
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr)
 {
     uint64_t d = 0;
@@ -82,7 +87,7 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr)
     d |= (uint64_t)(16 >> 4) << 16;          // leading byte offset (unused for swizzled K-major)
     d |= (uint64_t)((8 * SWZ_BYTES) >> 4) << 32;   // stride byte offset
     d |= (uint64_t)1 << 46;                  // descriptor version
-    d |= (uint64_t)(SWZ_BYTES == 128 ? 2 : 4) << 61;
+    d |= (uint64_t)(SWZ_BYTES == 128 ? 2 : SWZ_BYTES == 64 ? 4 : 6) << 61;
     return d;
 }
 
@@ -287,7 +292,7 @@ EncodeTiled encode_fn()
     return fn;
 }
 
-// a row-major rows x cols (floats, row pitch pitch_f) matrix, box of BKF floats x box_rows rows, 128B swizzle
+// a row-major rows x cols (floats, row pitch pitch_f) matrix, box of BKF floats x box_rows rows, swizzled rows
 int make_map(CUtensorMap *m, const float *ptr, long rows, long cols, long pitch_f, int box_rows)
 {
     EncodeTiled enc = encode_fn();
@@ -298,7 +303,8 @@ int make_map(CUtensorMap *m, const float *ptr, long rows, long cols, long pitch_
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)ptr, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     SWZ_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     SWZ_BYTES == 128 ? CU_TENSOR_MAP_SWIZZLE_128B :
+                     SWZ_BYTES == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) { m25_set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return M25_ECUDA; }

@@ -38,9 +38,13 @@ PREDICT_AFTER = 6            # iterations after which a fresh factor's refinemen
 MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
 REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
 REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most
-REUSE_GIVE_UP = (12, 100.0)  # a reused factor's GMRES ends once, after this many steps, its last steps' rate cannot
-                             # bring the residual within this factor of the tolerance by its cap (a fresh LU follows;
-                             # measured: from 8 steps with 10x, attempts that converged in 25 were cut off)
+REUSE_GIVE_UP = (10, 0.05)   # a reused factor's GMRES ends from step 10 where a residual is still above 5% of |b| (a
+                             # fresh LU follows). Rules that projected the rate of the last few steps to the cap were
+                             # measured and dropped: GMRES plateaus and then speeds up, and they cut off attempts that
+                             # converged in 25 steps
+FRESH_STAGNATION = (10, 0.5)  # a fresh factor's GMRES ends at step 10 where a residual has not halved since step 1
+                             # (measured on the routed board: at 0.5 GHz it stays at 2e-3 for all 30 steps; at 0.67 GHz
+                             # it is 5x lower by step 10 and converges at 27)
 DOUBLE_REACH = float(np.log(1.5))  # |ln f / f0| within which the kept double factor preconditions a double solve
 
 
@@ -443,7 +447,7 @@ class DirectSolver:
         rec = self._factor_c64(Z64)
         M = lambda R: self._timed('refine_precond', lambda: self._solve_c64(rec, R))
         e0, t = self._mark(), time.perf_counter()
-        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, FRESH_STALL, predict=False)
+        Y, ok, rel = self.refine(A, B, M, MIXED_MAX_ITER, FRESH_STALL, predict=False, stagnate=FRESH_STAGNATION)
         self._learn_t_iter((time.perf_counter() - t) / max(1, max(self.iters, default=1)))
         self._t('refine', e0)
         if ok:
@@ -527,11 +531,11 @@ class DirectSolver:
         return out
 
     # ---- the refinement: batched right-preconditioned GMRES (fast.py:658-663, 1437-1500) -----------------------------
-    def refine(self, A, B, M, restart, stall=None, predict=True, give_up=None):
+    def refine(self, A, B, M, restart, stall=None, predict=True, give_up=None, stagnate=None):
         """fast.py:658-663: GMRES to MIXED_RTOL, one cycle of at most `restart` iterations; (Y, converged, largest
         relative residual of B - A Y)."""
         Y, self.iters = self.gmres_batched(A, B, M, rtol=MIXED_RTOL, restart=restart, stall=stall, predict=predict,
-                                           give_up=give_up)
+                                           give_up=give_up, stagnate=stagnate)
         R = B - A(Y)
         rn = np.sqrt(np.abs(self._dotc(R, R)))
         bn = np.sqrt(np.abs(self._dotc(B, B)))
@@ -539,7 +543,7 @@ class DirectSolver:
         self.residual = rel
         return Y, bool(np.isfinite(rel).all() and (rel <= 100 * MIXED_RTOL).all()), float(rel.max())
 
-    def gmres_batched(self, A, B, M, rtol=1e-6, restart=30, stall=None, predict=True, give_up=None):
+    def gmres_batched(self, A, B, M, rtol=1e-6, restart=30, stall=None, predict=True, give_up=None, stagnate=None):
         """Right-preconditioned GMRES on A Y = B for the k columns of B at once, one cycle from Y = 0, the role of
         the reference's gmres_batched (fast.py:1437-1500) as its callers use it (maxiter 1, fast.py:1053):
 
@@ -554,6 +558,10 @@ class DirectSolver:
           FRESH_STALL rule, fast.py:256); with predict, after PREDICT_AFTER steps a column whose geometric rate
           so far would leave it 10x above the tolerance at the last step also ends it (the caller will solve in
           double precision: the steps that remain would be lost);
+        - give_up = (n, x): from step n a column whose residual is still above x |b| ends the iteration (a
+          reused factor that will not converge within its cap gives way to a fresh one sooner);
+        - stagnate = (n, x): at step n a column whose residual is above x times its residual after the first step
+          ends the iteration (a fresh factor too weak to precondition: the caller solves in double precision);
         - Y = sum_j Z_j y_j, one device product per step used.
         Returns (Y, iterations per column)."""
         N, k = B.shape
@@ -588,10 +596,12 @@ class DirectSolver:
             if done.all():
                 break
             act = ~done
-            if give_up is not None and j + 1 >= give_up[0] and j + 1 < restart:
-                rate = (res[act] / np.maximum(hist[-4][act], SMALL)) ** (1.0 / 3)
-                if (res[act] * rate ** (restart - j - 1) > give_up[1] * rtol * bn[act]).any():
-                    break
+            if give_up is not None and j + 1 >= give_up[0] and j + 1 < restart and \
+                    (res[act] > give_up[1] * bn[act]).any():
+                break
+            if stagnate is not None and j + 1 == stagnate[0] and j + 1 < restart and \
+                    (res[act] > stagnate[1] * hist[1][act]).any():
+                break
             if stall is not None and j + 1 >= stall[0] and (res[act] > stall[1] * bn[act]).any():
                 break
             if stall is not None and predict and j + 1 >= PREDICT_AFTER:

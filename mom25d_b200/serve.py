@@ -40,7 +40,8 @@ class Request:
 
     def __init__(self, rid, board, f, arrival=0.0, far=None):
         self.rid, self.board, self.f, self.arrival = rid, board, float(f), float(arrival)
-        self.far = far                  # Z with the far part at f already filled (the batched sweep), or None
+        self.far = far                  # Z with the far part at f already filled (the batched sweep), a callable
+                                        # returning it when ready, or None
         self.start = self.done = None
         self.S = self.error = self.slot = self.path = None
         self.iters = []
@@ -141,7 +142,7 @@ class Server:
         with torch.cuda.stream(stream):
             try:
                 if far is not None:
-                    stream.wait_stream(torch.cuda.default_stream())    # (filled on the default stream)
+                    stream.wait_stream(torch.cuda.default_stream())    # (filled and synchronised before)
                 try:
                     X = ds.solve_direct(f, geo.excitation(), precision=self.precision, far=far)
                 except SolveFailed:                     # (sim.py's rule: the frequency again in double precision)
@@ -189,9 +190,11 @@ class Server:
                     return
                 r.start = clock() - t0
                 try:
-                    r.S, info = self._solve(slot, r.board, r.f) if r.far is None else \
-                        self._solve(slot, r.board, r.f, far=r.far)
+                    far = r.far() if callable(r.far) else r.far        # (a callable: wait for the fill)
                     r.far = None
+                    r.S, info = self._solve(slot, r.board, r.f) if far is None else \
+                        self._solve(slot, r.board, r.f, far=far)
+                    del far
                     r.path, r.iters = info.get('path'), info.get('iters', [])
                 except Exception as e:                   # reported on the request; the loop keeps serving
                     r.error = f"{type(e).__name__}: {e}"
