@@ -285,6 +285,11 @@ int m25_cgemm_update_tf32(float *d_C, long ld, int M, int N, int K, const float 
                           size_t work_bytes, void *stream);
 /* 1 when the library carries the tensor-core (tcgen05) update. */
 int m25_umma_available(void);
+/* The tensor-core update's work split (no counterpart in the reference): `tiles` = 1 gives one output tile a CTA,
+ * two CTAs an SM; more gives runs of that many consecutive tiles a CTA, one CTA an SM, with two tensor-memory
+ * accumulators so each tile's epilogue runs under the next tile's MMAs - for updates of at least min_tiles tiles
+ * (min_tiles < 0: two an SM). M25_UMMA_TPC in the environment overrides `tiles`. */
+int m25_set_umma_tiles(int tiles, int min_tiles);
 
 /* ---- small helpers ------------------------------------------------------------------------------------------------ */
 /* J_n(z) elementwise for complex z, n = 0, 1, 2 (bessel_jn_complex, mom25d_core.cpp:1545-1558). */

@@ -15,6 +15,9 @@
 // Every wait is bounded: on time-out the kernel records M25_DEV_TIMEOUT, waits (bounded) for the MMAs it issued,
 // frees its tensor memory and returns. No multicast anywhere (single-GPU code, one CTA per cluster).
 #include <cuda.h>
+#include <algorithm>
+#include <cstdlib>
+
 #include "common.cuh"
 
 int *m25_dev_err_word();
@@ -34,6 +37,7 @@ namespace {
 #endif
 constexpr int BM = 128, BN = 256, BKF = M25_UMMA_BKF;
 constexpr int STAGES = M25_UMMA_STAGES;
+constexpr int RASTER = 16;                           // row tiles a group of the tile order
 constexpr int SWZ_BYTES = BKF * 4;                   // the swizzle span: one K row of a stage
 static_assert(SWZ_BYTES == 32 || SWZ_BYTES == 64 || SWZ_BYTES == 128, "32B, 64B or 128B swizzle");
 constexpr int A_BYTES = BM * BKF * 4, B_BYTES = BN * BKF * 4;
@@ -129,7 +133,19 @@ __global__ void __launch_bounds__(128, CTAS_PER_SM) k_umma_update(float *C, long
     __shared__ int abort_flag;
     __shared__ int issued_k, consumed_k;                           // stages loaded / multiplied (abort clean-up)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    // tile order: CTAs in launch order walk down a group of RASTER row tiles, then on to the next column tile, so the
+    // CTAs in flight (two an SM) cover a block of about RASTER x 18 tiles whose A' and B' slabs stay in L2; in plain
+    // order they swept every column tile of a row tile and read B' from DRAM again for every few row tiles
+    int m0, n0;
+    {
+        const int nm = gridDim.y, nn = gridDim.x;
+        const int pid = blockIdx.y * nn + blockIdx.x;
+        const int group = pid / (RASTER * nn), first = group * RASTER;
+        const int rows = min(nm - first, RASTER);
+        const int in_group = pid - group * RASTER * nn;
+        m0 = (first + in_group % rows) * BM;
+        n0 = (in_group / rows) * BN;
+    }
 
     if (threadIdx.x == 0) {
         abort_flag = 0;
@@ -236,6 +252,187 @@ __global__ void __launch_bounds__(128, CTAS_PER_SM) k_umma_update(float *C, long
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+// ---- the same update with a short run of tiles a CTA and two tensor-memory accumulators --------------------------
+// One CTA an SM (four 48 KB stages: 193 KB of shared memory; 2 x 256 tensor-memory columns), CTAs of six warps:
+//   warp 0 lane 0   TMA producer over the CTA's tiles and their K chunks (one running chunk count: the stage ring
+//                   carries on from tile to tile)
+//   warp 1 lane 0   MMA issuer: tile i accumulates in tensor memory columns (i & 1) x 256, after the epilogue has
+//                   released that half (tempty); the tile's last commit signals the epilogue (tfull)
+//   warps 2 - 5     epilogue: warp w reads accumulator lanes 32 (w mod 4) .. + 31 of tile i while the MMAs of tile
+//                   i + 1 run in the other half, then releases the half (one arrival a warp)
+// A CTA takes `tpc` consecutive tiles of the rasterised order and exits: short-lived enough that the LU's panel
+// kernel (a cooperative launch on the other stream) still finds SMs, long enough that all but the last tile's
+// epilogue run under MMAs. Every wait is bounded as in k_umma_update; on a time-out the CTA records
+// M25_DEV_TIMEOUT, waits (bounded) for its loads and MMAs in flight, frees its tensor memory and returns.
+constexpr int P_STAGES = 4;
+constexpr int P_SMEM_BYTES = P_STAGES * STAGE_BYTES + 1024 + 256;
+constexpr unsigned P_TMEM_COLS = 512;
+static_assert(P_SMEM_BYTES <= 227 * 1024, "four stages in shared memory");
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void raster_tile(int pid, int nm, int nn, int &m0, int &n0)
+{
+    const int group = pid / (RASTER * nn), first = group * RASTER;
+    const int rows = min(nm - first, RASTER);
+    const int in_group = pid - group * RASTER * nn;
+    m0 = (first + in_group % rows) * BM;
+    n0 = (in_group / rows) * BN;
+}
+
+__global__ void __launch_bounds__(192, 1) k_umma_runs(float *C, long ldc_f, int Mp, int Nc, int kchunks, int tpc,
+                                                       int nm, int nn,
+                                                       const __grid_constant__ CUtensorMap mAhi,
+                                                       const __grid_constant__ CUtensorMap mAlo,
+                                                       const __grid_constant__ CUtensorMap mBhi,
+                                                       const __grid_constant__ CUtensorMap mBlo, int *err)
+{
+    extern __shared__ unsigned char smem_raw[];
+    const uint32_t base_raw = smem_u32(smem_raw);
+    const uint32_t base = (base_raw + 1023) & ~1023u;
+    const uint32_t bars = base + P_STAGES * STAGE_BYTES;
+    // full[s] at bars + 8 s, empty[s] at bars + 32 + 8 s, tfull[a] at bars + 64 + 8 a, tempty[a] at bars + 80 + 8 a,
+    // done at bars + 96, the tensor-memory address at bars + 104
+    const uint32_t full0 = bars, empty0 = bars + 8 * P_STAGES, tfull0 = bars + 16 * P_STAGES,
+                   tempty0 = tfull0 + 16, done = tempty0 + 16;
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(smem_raw + (done + 8 - base_raw));
+    __shared__ int abort_flag;
+    __shared__ int issued_k, consumed_k;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntiles = nm * nn;                                    // the tile grid: nm row tiles x nn column tiles
+    const int t0 = blockIdx.x * tpc, t1 = min(ntiles, t0 + tpc);
+
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        for (int st = 0; st < P_STAGES; ++st) { mbar_init(full0 + 8 * st, 1); mbar_init(empty0 + 8 * st, 1); }
+        for (int a = 0; a < 2; ++a) { mbar_init(tfull0 + 8 * a, 1); mbar_init(tempty0 + 8 * a, 4); }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issued_k = 0;
+        consumed_k = 0;
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32((const void *)tmem_slot)), "r"(P_TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    volatile int *abort = &abort_flag;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        int kg = 0;
+        for (int t = t0; t < t1 && !*abort; ++t) {
+            int m0, n0;
+            raster_tile(t, nm, nn, m0, n0);
+            for (int kc = 0; kc < kchunks; ++kc, ++kg) {
+                const int st = kg % P_STAGES;
+                if (kg >= P_STAGES && !mbar_wait(empty0 + 8 * st, ((kg / P_STAGES) - 1) & 1, abort)) break;
+                const uint32_t sb = base + st * STAGE_BYTES;
+                mbar_expect_tx(full0 + 8 * st, STAGE_BYTES);
+                const int x = kc * BKF;
+                tma_load_2d(sb, &mAhi, x, m0, full0 + 8 * st);
+                tma_load_2d(sb + A_BYTES, &mAlo, x, m0, full0 + 8 * st);
+                tma_load_2d(sb + 2 * A_BYTES, &mBhi, x, n0, full0 + 8 * st);
+                tma_load_2d(sb + 2 * A_BYTES + B_BYTES, &mBlo, x, n0, full0 + 8 * st);
+                issued_k = kg + 1;
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        int kg = 0, i = 0;
+        for (int t = t0; t < t1 && !*abort; ++t, ++i) {
+            const int a = i & 1, use = i >> 1;
+            if (use > 0 && !mbar_wait(tempty0 + 8 * a, (use - 1) & 1, abort)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d = tmem + (uint32_t)(a * 256);
+            bool ok = true;
+            for (int kc = 0; kc < kchunks; ++kc, ++kg) {
+                const int st = kg % P_STAGES;
+                if (!mbar_wait(full0 + 8 * st, (kg / P_STAGES) & 1, abort)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sb = base + st * STAGE_BYTES;
+                const uint32_t aH = sb, aL = sb + A_BYTES, bH = sb + 2 * A_BYTES, bL = sb + 2 * A_BYTES + B_BYTES;
+#pragma unroll
+                for (int k = 0; k < BKF / 8; ++k) {
+                    const uint32_t off = k * 32;
+                    umma_tf32(d, sdesc(aL + off), sdesc(bH + off), (kc > 0 || k > 0) ? 1u : 0u);
+                    umma_tf32(d, sdesc(aH + off), sdesc(bL + off), 1u);
+                    umma_tf32(d, sdesc(aH + off), sdesc(bH + off), 1u);
+                }
+                umma_commit(empty0 + 8 * st);
+                consumed_k = kg + 1;
+            }
+            if (!ok) break;
+            umma_commit(tfull0 + 8 * a);                     // the tile's accumulator is complete
+        }
+        umma_commit(done);                                   // (every MMA issued so far complete)
+    } else if (warp >= 2) {
+        // epilogue: warp w reads tensor-memory lanes 32 (w mod 4) .. + 31
+        const int q = warp & 3;
+        int i = 0;
+        for (int t = t0; t < t1; ++t, ++i) {
+            const int a = i & 1, use = i >> 1;
+            const bool ok = mbar_wait(tfull0 + 8 * a, use & 1, abort);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!__all_sync(0xffffffffu, ok && !*abort)) break;          // warp-uniform: tcgen05.ld is .sync.aligned
+            int m0, n0;
+            raster_tile(t, nm, nn, m0, n0);
+            const int row = m0 + q * 32 + lane;
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t v[32];
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * 256 + c0);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+                             "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                               "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+                               "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+                               "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (row < Mp) {
+                    float cv[32];
+                    float *pc = C + (size_t)(n0 + c0) * ldc_f + row;
+                    const int nv = min(32, Nc - (n0 + c0));
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) cv[j] = j < nv ? __ldcs(pc + (size_t)j * ldc_f) : 0.f;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (j < nv) __stcs(pc + (size_t)j * ldc_f, cv[j] - __uint_as_float(v[j]));
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty0 + 8 * a);     // this half may take the next tile's accumulation
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile int never = 0;
+        if (*abort) {
+            dev_error(err, M25_DEV_TIMEOUT);
+            // loads still in flight would land in this CTA's shared memory after it exits: wait for them (bounded)
+            for (int kc = consumed_k; kc < issued_k; ++kc)
+                mbar_wait(full0 + 8 * (kc % P_STAGES), (kc / P_STAGES) & 1, &never);
+        }
+        never = 0;
+        mbar_wait(done, 0, &never);                          // the MMAs issued (they read shared, write tensor memory)
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P_TMEM_COLS) : "memory");
+}
+
 // A' (2M x Kp floats, row-major, hi and lo) from L (M x K complex, column-major, lda): rows 2m / 2m+1 hold
 // [Lr, -Li] / [Li, Lr] for every k; columns 2K .. Kp zero. A 32 x 32 (m, k) tile through shared memory so both the
 // read (along m) and the write (along k) are coalesced.
@@ -313,6 +510,29 @@ int make_map(CUtensorMap *m, const float *ptr, long rows, long cols, long pitch_
 
 }  // namespace
 
+// Tiles a CTA of the tensor-core update: 1 runs k_umma_update (one tile a CTA, two CTAs an SM), more runs k_umma_runs
+// with that many consecutive tiles a CTA, for updates of at least `min_tiles` tiles (default two an SM; smaller ones
+// keep one tile a CTA). M25_UMMA_TPC in the environment overrides the count.
+static int g_umma_tpc = 1, g_umma_min = -1;
+
+extern "C" int m25_set_umma_tiles(int tiles, int min_tiles)
+{
+    M25_REQUIRE(tiles >= 1 && tiles <= 64, "m25_set_umma_tiles: 1 to 64 tiles a CTA");
+    g_umma_tpc = tiles;
+    g_umma_min = min_tiles;
+    return M25_OK;
+}
+
+static int umma_tiles_per_cta(int ntiles)
+{
+    int t = g_umma_tpc;
+    if (const char *e = getenv("M25_UMMA_TPC")) t = std::max(1, std::min(64, atoi(e)));
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int need = g_umma_min >= 0 ? g_umma_min : 2 * sms;
+    return (t > 1 && ntiles >= need) ? t : 1;
+}
+
 size_t m25_umma_workspace(int n, int nb)
 {
     (void)nb;
@@ -343,15 +563,28 @@ int m25_umma_trailing(float *C, long lda, int M, int Nc, int K, const float *L21
     if ((rc = make_map(&mAlo, Alo, 2L * M, Kp, Kp, BM))) return rc;
     if ((rc = make_map(&mBhi, Bhi, Nc, Kp, Kp, BN))) return rc;
     if ((rc = make_map(&mBlo, Blo, Nc, Kp, Kp, BN))) return rc;
-    static bool attr = false;
-    if (!attr) {
-        M25_CHECK(cudaFuncSetAttribute(k_umma_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        attr = true;
+    const int nm = (2 * M + BM - 1) / BM, nn = (Nc + BN - 1) / BN, ntiles = nm * nn;
+    const int tpc = umma_tiles_per_cta(ntiles);
+    if (tpc <= 1) {                                          // one tile a CTA, two CTAs an SM
+        static bool attr = false;
+        if (!attr) {
+            M25_CHECK(cudaFuncSetAttribute(k_umma_update, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+            attr = true;
+        }
+        dim3 grid(nn, nm);
+        k_umma_update<<<grid, 128, SMEM_BYTES, s>>>(C, 2 * lda, 2 * M, Nc, Kp / BKF, mAhi, mAlo, mBhi, mBlo,
+                                                    m25_dev_err_word());
+        M25_LAUNCH_CHECK("k_umma_update");
+        return M25_OK;
     }
-    dim3 grid((Nc + BN - 1) / BN, (2 * M + BM - 1) / BM);
-    k_umma_update<<<grid, 128, SMEM_BYTES, s>>>(C, 2 * lda, 2 * M, Nc, Kp / BKF, mAhi, mAlo, mBhi, mBlo,
-                                                m25_dev_err_word());
-    M25_LAUNCH_CHECK("k_umma_update");
+    static bool pattr = false;
+    if (!pattr) {
+        M25_CHECK(cudaFuncSetAttribute(k_umma_runs, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM_BYTES));
+        pattr = true;
+    }
+    k_umma_runs<<<(ntiles + tpc - 1) / tpc, 192, P_SMEM_BYTES, s>>>(C, 2 * lda, 2 * M, Nc, Kp / BKF, tpc, nm, nn, mAhi,
+                                                                     mAlo, mBhi, mBlo, m25_dev_err_word());
+    M25_LAUNCH_CHECK("k_umma_runs");
     return M25_OK;
 }
 
