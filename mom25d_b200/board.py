@@ -33,17 +33,40 @@ class Layer:
         return self.er * (1 - 1j * self.tand)
 
 
+def check_stack(stack):
+    """Raises NotImplementedError for a stack the device Green network does not model: an open bottom, PEC planes
+    inside the stack, or layers whose permittivity depends on f (the reference's LayerStack(bottom='open',
+    bottom_er, pec=(...)) and Layer(fref=...), multilayer.py:96-111, 118-127). Takes this module's LayerStack or
+    the reference's own, so that such a stack is refused at the seam instead of solved as a grounded one."""
+    bottom = getattr(stack, 'bottom', 'pec')
+    planes = tuple(getattr(stack, 'pec', ()) or ())
+    if bottom != 'pec':
+        raise NotImplementedError("the layer stack has an open bottom (bottom=%r): the device Green network models "
+                                  "a PEC ground at z = 0 only" % (bottom,))
+    if planes:
+        raise NotImplementedError("the layer stack has PEC planes at interfaces %s: the device Green network models "
+                                  "no planes inside the stack" % (list(planes),))
+    if getattr(stack, 'dispersive', False):
+        raise NotImplementedError("the layer stack has wideband (frequency-dependent) layers: the device Green "
+                                  "network takes constant permittivities")
+
+
 class LayerStack:
     """Dielectric layers bottom -> top over a PEC ground (interface 0, z = 0); interface k is the top of layer k.
     top: 'open' (a half-space of top_er above) or 'pec' (a cover on interface N). Mirrors multilayer.py:90-250
-    for the stacks the hot path is exercised on (no PEC planes inside the stack, no open bottom)."""
+    for grounded stacks: the reference's bottom='open' and internal PEC planes (pec=...) are accepted as arguments
+    and refused with NotImplementedError (check_stack)."""
 
-    def __init__(self, layers, top='open', top_er=1.0):
+    def __init__(self, layers, top='open', top_er=1.0, bottom='pec', bottom_er=1.0, pec=()):
         if top not in ('open', 'pec'):
             raise ValueError("top: 'open' or 'pec'")
+        if bottom not in ('open', 'pec'):
+            raise ValueError("bottom: 'open' or 'pec'")
         self.layers, self.top, self.top_er = list(layers), top, float(top_er)
         self.N = len(self.layers)
-        self.bottom = 'pec'
+        self.bottom, self.bottom_er = bottom, float(bottom_er)
+        self.pec = tuple(sorted({int(k) for k in pec}))
+        check_stack(self)
         self.z = np.concatenate([[0.0], np.cumsum([l.h for l in self.layers])])
 
     def eps(self, j):
@@ -293,6 +316,9 @@ class Board:
     near_fac: float = 5.0
     name: str = 'board'
     rects: dict = field(default_factory=dict)     # interface -> [(x0, y0, x1, y1)]: the copper, for on-metal tests
+
+    def __post_init__(self):
+        check_stack(self.stack)
 
 
 def _on_copper(rects, x, y, tol=1e-9):

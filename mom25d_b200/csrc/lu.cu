@@ -1590,6 +1590,8 @@ static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B,
     R *W1 = (R *)(aux + ow), *W2 = W1 + 2 * (size_t)n * 16;
     const int nb = (n + TB - 1) / TB;
     int *flags = (int *)(aux + of), *epoch = flags + 2 * nb;
+    // CTAs of the persistent solves: one an SM (measured at N = 18,788, complex64, 8 columns: 3.4 ms with 148 CTAs,
+    // 4.8 / 5.3 / 6.6 ms with 100 / 74 / 59, each owning more consecutive blocks)
     const int G = std::max(1, std::min(sm_count(), nb));
     const size_t sm = trsv_smem<R>(n, G);
     M25_REQUIRE(sm <= 200 * 1024, "m25_getrs_aux: n too large for the persistent solve");
