@@ -402,20 +402,153 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel(R *A, long lda, int n, 
     }
 }
 
-// interchanges ipiv[r0 .. r0 + nsw) applied in order to the columns [c0, c1): one thread per column
-template <typename R>
-__global__ void k_laswp(R *A, long lda, int n, int r0, int nsw, const int *ipiv, long c0, long c1)
+// ---- interchanges as one permutation ----------------------------------------------------------------------------
+// The interchanges of rows r0 + i and p_i = ipiv[r0 + i], i = 0 .. nsw - 1, applied in order (LAPACK's laswp), with
+// partial pivoting's p_i >= r0 + i, are one permutation of the rows they touch, and every row's final content has a
+// closed form. Row r0 + i is not touched after step i, so it ends with what row p_i held just before step i. A row
+// x >= r0 + i holds, before step i, its own content unless an earlier step h moved something into it (p_h = x), and
+// then what row r0 + h held before step h. With B(i) = what row r0 + i holds before step i:
+//   B(i)       = B(h) for the last h < i with p_h = r0 + i, else row r0 + i's own content;
+//   row r0 + i ends with B(h) for the last h < i with p_h = p_i, else row p_i's own content;
+//   a row x >= r0 + nsw ends with B(h) for the last h with p_h = x.
+// B's links go to smaller indices, so log2(nsw) rounds of pointer jumping find each chain's root. swap_plan builds
+// this in shared memory with the CTA's threads: dst[e] / src[e], e < m: after the interchanges row dst[e] holds what
+// row src[e] held before them. The first nsw entries are rows r0 .. r0 + nsw in order (some unchanged), then the rows
+// below that moved. A pivot out of range (p_i < r0 + i or >= n) is recorded as M25_DEV_INDEX and taken as none.
+#define PLAN_MAX 256
+static_assert(NB2 <= PLAN_MAX, "an outer panel's interchanges make one plan");
+struct SwapPlan {
+    int piv[PLAN_MAX];
+    int jump[2][PLAN_MAX];
+    int low[PLAN_MAX];                 // the source row for a moved row below, else -1
+    int dst[2 * PLAN_MAX], src[2 * PLAN_MAX];
+    int m;
+};
+
+__device__ void swap_plan(const int *ipiv, int r0, int nsw, int n, SwapPlan &P, int *err)
 {
-    long c = c0 + blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (c >= c1) return;
-    R *col = A + 2 * (size_t)c * lda;
-    for (int j = 0; j < nsw; ++j) {
-        int p = ipiv[r0 + j], r = r0 + j;
-        if (p != r && p >= 0 && p < n) {
-            cpx<R> a = ldc<R>(col, r), b = ldc<R>(col, p);
-            stc<R>(col, r, b); stc<R>(col, p, a);
+    const int T = blockDim.x, t = threadIdx.x;
+    for (int i = t; i < nsw; i += T) {
+        int p = ipiv[r0 + i];
+        if (p < r0 + i || p >= n) {
+            dev_error(err, M25_DEV_INDEX);
+            p = r0 + i;
+        }
+        P.piv[i] = p;
+    }
+    __syncthreads();
+    for (int i = t; i < nsw; i += T) {                     // B's link: the last h < i with p_h = r0 + i, else i
+        int last = i;
+        for (int h = 0; h < i; ++h)
+            if (P.piv[h] == r0 + i) last = h;
+        P.jump[0][i] = last;
+    }
+    __syncthreads();
+    int cur = 0;
+    for (int s = 1; s < nsw; s <<= 1) {
+        for (int i = t; i < nsw; i += T) P.jump[cur ^ 1][i] = P.jump[cur][P.jump[cur][i]];
+        __syncthreads();
+        cur ^= 1;
+    }
+    for (int i = t; i < nsw; i += T) {
+        const int p = P.piv[i];
+        int last = -1;
+        bool later = false;
+        for (int h = 0; h < nsw; ++h)
+            if (P.piv[h] == p) {
+                if (h < i) last = h;
+                else if (h > i) later = true;
+            }
+        P.dst[i] = r0 + i;
+        P.src[i] = last >= 0 ? r0 + P.jump[cur][last] : p;
+        P.low[i] = (p >= r0 + nsw && !later) ? r0 + P.jump[cur][i] : -1;
+    }
+    __syncthreads();
+    if (t < 32) {                                          // the moved rows below, in order of i
+        int m = nsw;
+        for (int b = 0; b < nsw; b += 32) {
+            const int i = b + t;
+            const bool f = i < nsw && P.low[i] >= 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, f);
+            if (f) {
+                const int e = m + __popc(bal & ((1u << t) - 1u));
+                P.dst[e] = P.piv[i];
+                P.src[e] = P.low[i];
+            }
+            m += __popc(bal);
+        }
+        if (t == 0) P.m = m;
+    }
+    __syncthreads();
+}
+
+// The plan applied to up to COLS columns (cs[j] < 0: none) by a warp, Q entries a lane (P.m <= 32 Q): every source
+// of them read before any destination is written (the warp barrier orders the lanes' loads before their stores).
+// Entries e < top go to shared memory instead (xs[j * xcol + e * xrow]) when xs is given.
+template <typename R, int Q, int COLS>
+__device__ __forceinline__ void apply_plan(R *A, long lda, const long (&cs)[COLS], const SwapPlan &P, int lane,
+                                           cpx<R> *xs, int top, int xcol, int xrow)
+{
+    cpx<R> v[COLS][Q];
+#pragma unroll
+    for (int j = 0; j < COLS; ++j) {
+        if (cs[j] < 0) continue;
+        const R *col = A + 2 * (size_t)cs[j] * lda;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int e = lane + 32 * q;
+            if (e < P.m) v[j][q] = ldc<R>(col, P.src[e]);
         }
     }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < COLS; ++j) {
+        if (cs[j] < 0) continue;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int e = lane + 32 * q;
+            if (e < P.m) {
+                if (xs && e < top) xs[(size_t)j * xcol + (size_t)e * xrow] = v[j][q];
+                else stc<R>(A, (size_t)cs[j] * lda + P.dst[e], v[j][q]);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// a warp's columns k .. k + COLS of the two ranges [a0, a1), [b0, b1) (na = a1 - a0, nc in all), the plan applied
+template <typename R, int Q, int COLS>
+__device__ __forceinline__ void laswp_cols(R *A, long lda, const SwapPlan &P, long a0, long na, long b0, long nc,
+                                           int lane, long wid, long nw)
+{
+    for (long k = wid * COLS; k < nc; k += nw * COLS) {
+        long cs[COLS];
+#pragma unroll
+        for (int j = 0; j < COLS; ++j) {
+            const long kk = k + j;
+            cs[j] = kk >= nc ? -1 : kk < na ? a0 + kk : b0 + (kk - na);
+        }
+        apply_plan<R, Q, COLS>(A, lda, cs, P, lane, nullptr, 0, 0, 0);
+    }
+}
+
+// Interchanges on columns: the plan of rows r0 .. (nsw interchanges) on the columns [a0, a1) and [b0, b1), a warp a
+// few columns at a time. blockIdx.y = g > 0 shifts the rows, the interchange count (down) and [a0, a1) by g gs: the
+// interchanges of an outer panel's later panels applied to each earlier panel's columns in one launch.
+template <typename R>
+__global__ void __launch_bounds__(256) k_laswp_plan(R *A, long lda, int n, const int *ipiv, int r0, int nsw, long a0,
+                                                    long a1, long b0, long b1, int gs, int *err)
+{
+    __shared__ SwapPlan P;
+    const int g = blockIdx.y;
+    r0 += g * gs; nsw -= g * gs; a0 += (long)g * gs; a1 += (long)g * gs;
+    swap_plan(ipiv, r0, nsw, n, P, err);
+    const long na = a1 - a0, nc = na + (b1 - b0);
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const long wid = (long)blockIdx.x * wpb + (threadIdx.x >> 5), nw = (long)gridDim.x * wpb;
+    if (nsw <= 64) laswp_cols<R, 4, 4>(A, lda, P, a0, na, b0, nc, lane, wid, nw);
+    else if (nsw <= 128) laswp_cols<R, 8, 2>(A, lda, P, a0, na, b0, nc, lane, wid, nw);
+    else laswp_cols<R, 16, 1>(A, lda, P, a0, na, b0, nc, lane, wid, nw);
 }
 
 // A[k0 .. k0 + jb, c0 .. c1) = L11^-1 A[k0 .. k0 + jb, c0 .. c1), L11 = A[k0 .., k0 ..] unit lower (jb <= NB), in
@@ -451,23 +584,30 @@ __global__ void __launch_bounds__(256) k_trsm(R *A, long lda, int k0, int jb, lo
         for (int k = g; k < jb; k += 4) stc<R>(A, (size_t)c * lda + k0 + k, X[k * 64 + cl]);
 }
 
+
 // The same for a full panel (jb = NB = 64) without a barrier inside the substitution: a warp solves 32
 // columns, one a lane, the lane's column in registers (64 complex), L11 in shared memory read as broadcasts. The
 // columns are staged through shared memory (a column's stride NB + 1: the lanes' reads of their own columns fall in
 // different banks) so that every global load and store is a warp's 256 contiguous bytes. The arithmetic and its
 // order are those of k_trsm (row i's multiple subtracted from the rows below, i ascending).
-template <typename R, int T64_WARPS>
-__global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64(R *A, long lda, int k0, long c0, long c1)
+// With SWAP, the panel's own interchanges (ipiv[k0 .. k0 + NB)) are applied to the columns as they are loaded: the
+// solved rows come from the plan's sources, and the rows below that move are written back directly (the separate
+// interchange launch folded into this one).
+template <typename R, int T64_WARPS, bool SWAP>
+__global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64(R *A, long lda, int k0, long c0, long c1, const int *ipiv,
+                                                           int n, int *err)
 {
     typedef cpx<R> C;
     typedef typename vec2_of<R>::type V;
     constexpr int XS = NB + 1;
     extern __shared__ __align__(16) unsigned char t64_raw[];
+    __shared__ SwapPlan P;
     C *L = reinterpret_cast<C *>(t64_raw);                   // L[i * NB + k] = L11(k, i)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     C *Xs = L + NB * NB + (size_t)w * 32 * XS;
     const V *A2 = reinterpret_cast<const V *>(A);
     static_assert(NB * NB % (8 * 32 * T64_WARPS) == 0, "L11 in whole batches");
+    if (SWAP) swap_plan(ipiv, k0, NB, n, P, err);
     for (int e0 = threadIdx.x; e0 < NB * NB; e0 += 8 * 32 * T64_WARPS) {     // 8 loads in flight a thread
         V v[8];
 #pragma unroll
@@ -479,7 +619,15 @@ __global__ void __launch_bounds__(32 * T64_WARPS) k_trsm64(R *A, long lda, int k
         for (int q = 0; q < 8; ++q) L[e0 + q * 32 * T64_WARPS] = mk<R>(v[q].x, v[q].y);
     }
     const long cbase = c0 + ((long)blockIdx.x * T64_WARPS + w) * 32;
-    for (int c8 = 0; c8 < 32; c8 += 8) {                    // 16 loads in flight a lane
+    if (SWAP) {                                             // 4 rows x 8 (4) columns of loads in flight a lane
+        constexpr int SC = sizeof(R) == 4 ? 8 : 4;
+        for (int c8 = 0; c8 < 32; c8 += SC) {
+            long cs[SC];
+#pragma unroll
+            for (int j = 0; j < SC; ++j) cs[j] = cbase + c8 + j < c1 ? cbase + c8 + j : -1;
+            apply_plan<R, 4, SC>(A, lda, cs, P, lane, Xs + c8 * XS, NB, XS, 1);
+        }
+    } else for (int c8 = 0; c8 < 32; c8 += 8) {             // 16 loads in flight a lane
         V v[8][2];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -544,6 +692,80 @@ template <typename R> constexpr int t64_warps() { return sizeof(R) == 4 ? 4 : 2;
 template <typename R> constexpr size_t t64_smem()
 {
     return sizeof(cpx<R>) * (NB * NB + (size_t)t64_warps<R>() * 32 * (NB + 1));
+}
+
+// U12 of a whole outer panel in one launch: rows [K0, K0 + JB) (JB <= NB2) of the columns [c0, c1), after the outer
+// panel's interchanges (ipiv[K0 .. K0 + JB), applied as a plan; the rows below that move written back directly),
+// U12 = L11^-1 A12 with L11 = A[K0 .., K0 ..] unit lower. TO_COLS columns a CTA of 256 threads (a warp a column),
+// their JB rows in shared memory. By 64-row blocks: the diagonal block of L11 staged in shared memory, each warp
+// solves its column's 64 rows (two rows a lane in registers, the solved value passed by shuffle), then every thread
+// takes a row below the block and subtracts the block's multiples from it for all the CTA's columns (L read from
+// the factor, coalesced across the threads). Each entry takes its terms x -= L(k, i) x_i in ascending i, as a
+// forward substitution does; FP32 (FP64) on the CUDA cores throughout.
+#define TO_COLS 8
+#define TO_THREADS 256
+static_assert(TO_COLS * 32 == TO_THREADS, "a warp a column");
+template <typename R> constexpr size_t to_smem() { return sizeof(cpx<R>) * ((size_t)NB2 * TO_COLS + NB * (NB + 1)); }
+
+template <typename R>
+__global__ void __launch_bounds__(TO_THREADS) k_trsm_outer(R *A, long lda, int n, int K0, int JB, const int *ipiv,
+                                                           long c0, long c1, int *err)
+{
+    typedef cpx<R> C;
+    extern __shared__ __align__(16) unsigned char to_raw[];
+    __shared__ SwapPlan P;
+    C *X = reinterpret_cast<C *>(to_raw);                 // X[r * TO_COLS + j]: row K0 + r of the CTA's column j
+    C *Lb = X + (size_t)NB2 * TO_COLS;                     // Lb[i * (NB + 1) + k] = L11(kb + k, kb + i)
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const long cw = c0 + (long)blockIdx.x * TO_COLS + w;    // this warp's column
+    swap_plan(ipiv, K0, JB, n, P, err);
+    {
+        long cs[1] = {cw < c1 ? cw : -1};
+        apply_plan<R, 2 * PLAN_MAX / 32, 1>(A, lda, cs, P, lane, X + w, JB, 0, TO_COLS);
+        if (cw >= c1)
+            for (int r = lane; r < JB; r += 32) X[r * TO_COLS + w] = mk<R>(0, 0);
+    }
+    for (int kb = 0; kb < JB; kb += NB) {
+        const int jb = min(NB, JB - kb);
+        __syncthreads();                                   // (X complete; the previous block's Lb reads done)
+        for (int e = t; e < jb * jb; e += TO_THREADS) {
+            const int i = e / jb, k = e % jb;
+            Lb[i * (NB + 1) + k] = ldc<R>(A, (size_t)(K0 + kb + i) * lda + K0 + kb + k);
+        }
+        __syncthreads();
+        {                                                  // the diagonal block, warp w's column
+            C x0 = lane < jb ? X[(kb + lane) * TO_COLS + w] : mk<R>(0, 0);
+            C x1 = lane + 32 < jb ? X[(kb + lane + 32) * TO_COLS + w] : mk<R>(0, 0);
+            for (int i = 0; i < jb - 1; ++i) {
+                const C s = i < 32 ? x0 : x1;
+                C xi;
+                xi.x = __shfl_sync(0xffffffffu, s.x, i & 31);
+                xi.y = __shfl_sync(0xffffffffu, s.y, i & 31);
+                if (lane > i && lane < jb) cfms<R>(x0, Lb[i * (NB + 1) + lane], xi);
+                if (lane + 32 > i && lane + 32 < jb) cfms<R>(x1, Lb[i * (NB + 1) + lane + 32], xi);
+            }
+            if (lane < jb) X[(kb + lane) * TO_COLS + w] = x0;
+            if (lane + 32 < jb) X[(kb + lane + 32) * TO_COLS + w] = x1;
+        }
+        __syncthreads();
+        for (int r = kb + jb + t; r < JB; r += TO_THREADS) {   // the rows below the block
+            C x[TO_COLS];
+#pragma unroll
+            for (int j = 0; j < TO_COLS; ++j) x[j] = X[r * TO_COLS + j];
+            const R *lr = A + 2 * ((size_t)(K0 + kb) * lda + K0 + r);
+#pragma unroll 8
+            for (int i = 0; i < jb; ++i) {
+                const C l = ldc<R>(lr, (size_t)i * lda);
+#pragma unroll
+                for (int j = 0; j < TO_COLS; ++j) cfms<R>(x[j], l, X[(kb + i) * TO_COLS + j]);
+            }
+#pragma unroll
+            for (int j = 0; j < TO_COLS; ++j) X[r * TO_COLS + j] = x[j];
+        }
+    }
+    __syncthreads();
+    if (cw < c1)
+        for (int r = lane; r < JB; r += 32) stc<R>(A, (size_t)cw * lda + K0 + r, X[r * TO_COLS + w]);
 }
 
 // C (M x N) -= A (M x K) B (K x N), all column-major complex inside the factor (lda). A 128 x 64 tile per block of
@@ -1393,8 +1615,11 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     M25_CHECK(cudaMemsetAsync(pw.ll_cand, 0, ll_bytes, H));         // flags 0: no column's (they are column + 1)
     const size_t trsm_smem = sizeof(cpx<R>) * (NB * NB + NB * 64);
     M25_CHECK(cudaFuncSetAttribute(k_trsm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
-    M25_CHECK(cudaFuncSetAttribute(k_trsm64<R, t64_warps<R>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    M25_CHECK(cudaFuncSetAttribute(k_trsm64<R, t64_warps<R>(), false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)t64_smem<R>()));
+    M25_CHECK(cudaFuncSetAttribute(k_trsm64<R, t64_warps<R>(), true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)t64_smem<R>()));
+    M25_CHECK(cudaFuncSetAttribute(k_trsm_outer<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)to_smem<R>()));
     int smem_optin = 0, dev = 0;
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
@@ -1409,23 +1634,45 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     const int gcap = std::min(G, PANEL_THREADS);                     // a thread of each block reads a block's record
     M25_CHECK(cudaFuncSetAttribute(k_gemm_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem<R>()));
     M25_CHECK(cudaFuncSetAttribute(k_zgemm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)zdmma_smem()));
-    auto laswp = [&](int r0, int nsw, long c0, long c1, cudaStream_t cs) -> int {
-        if (c1 <= c0) return M25_OK;
-        k_laswp<R><<<(c1 - c0 + 127) / 128, 128, 0, cs>>>(A, lda, n, r0, nsw, ipiv, c0, c1);
-        M25_LAUNCH_CHECK("k_laswp");
+    // the interchanges ipiv[r0 .. r0 + nsw) on the columns [a0, a1) and [b0, b1); groups > 1: group g takes the
+    // rows, count and first range shifted by g gs
+    auto laswp = [&](int r0, int nsw, long a0, long a1, long b0, long b1, int gs, int groups, cudaStream_t cs) -> int {
+        const long nc = std::max(0L, a1 - a0) + std::max(0L, b1 - b0);
+        if (nc <= 0 || nsw <= 0) return M25_OK;
+        const long bx = std::min<long>((nc + 15) / 16, 4L * G);
+        k_laswp_plan<R><<<dim3((unsigned)bx, (unsigned)groups), 256, 0, cs>>>(A, lda, n, ipiv, r0, nsw, a0,
+                                                                             std::max(a0, a1), b0, std::max(b0, b1),
+                                                                             gs, err);
+        M25_LAUNCH_CHECK("k_laswp_plan");
         return M25_OK;
     };
-    auto trsm = [&](int k0, int jb, long c0, long c1, cudaStream_t cs) -> int {
+    // U12 rows k0 .. k0 + jb of the columns [c0, c1); swap: the panel's interchanges applied to them on the way
+    auto trsm = [&](int k0, int jb, long c0, long c1, bool swap, cudaStream_t cs) -> int {
         if (c1 <= c0) return M25_OK;
         if (jb == NB) {
             const long per = 32L * t64_warps<R>();
-            k_trsm64<R, t64_warps<R>()><<<(unsigned)((c1 - c0 + per - 1) / per), (unsigned)per, t64_smem<R>(), cs>>>(
-                A, lda, k0, c0, c1);
+            const unsigned grid = (unsigned)((c1 - c0 + per - 1) / per);
+            if (swap)
+                k_trsm64<R, t64_warps<R>(), true><<<grid, (unsigned)per, t64_smem<R>(), cs>>>(A, lda, k0, c0, c1,
+                                                                                               ipiv, n, err);
+            else
+                k_trsm64<R, t64_warps<R>(), false><<<grid, (unsigned)per, t64_smem<R>(), cs>>>(A, lda, k0, c0, c1,
+                                                                                                ipiv, n, err);
             M25_LAUNCH_CHECK("k_trsm64");
             return M25_OK;
         }
+        int rc2;
+        if (swap && (rc2 = laswp(k0, jb, c0, c1, 0, 0, 0, 1, cs))) return rc2;
         k_trsm<R><<<(c1 - c0 + 63) / 64, 256, trsm_smem, cs>>>(A, lda, k0, jb, c0, c1);
         M25_LAUNCH_CHECK("k_trsm");
+        return M25_OK;
+    };
+    // U12 of the whole outer panel [K0, K0 + JB) on the columns [c0, c1), its interchanges applied on the way
+    auto trsm_outer = [&](int K0, int JB, long c0, long c1, cudaStream_t cs) -> int {
+        if (c1 <= c0) return M25_OK;
+        k_trsm_outer<R><<<(unsigned)((c1 - c0 + TO_COLS - 1) / TO_COLS), TO_THREADS, to_smem<R>(), cs>>>(
+            A, lda, n, K0, JB, ipiv, c0, c1, err);
+        M25_LAUNCH_CHECK("k_trsm_outer");
         return M25_OK;
     };
     // C = A[r0 .., c0 ..] (M x Nc) -= A[r0 .., k0 .. k0 + K] A[k0 .. k0 + K, c0 ..]; the low-priority stream's
@@ -1481,34 +1728,29 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, H));
             }
             m25_note_launch();
-            if ((rc = laswp(k0, jb, K0, k0, H))) return rc;                // left, inside the outer panel
-            if ((rc = laswp(k0, jb, k0 + jb, KE, H))) return rc;           // the rest of the outer panel
-            if ((rc = trsm(k0, jb, k0 + jb, KE, H))) return rc;
+            if ((rc = trsm(k0, jb, k0 + jb, KE, true, H))) return rc;     // the rest of the outer panel
             // in FP32 on the CUDA cores, not 3xTF32: the columns of L pass through every update of their outer
             // panel, and the tensor-core error there (about 2^-22 a product against 2^-24) costs the factor its
             // use as a preconditioner near the low-frequency end (fresh LUs at 0.67 and 0.91 GHz of the routed
             // board no longer converged; the FP32 inner update costs 5 ms of 236 at N = 18,788)
             if ((rc = gemm(k0 + jb, n - k0 - jb, k0 + jb, KE - k0 - jb, k0, jb, false, H))) return rc;
         }
+        // each earlier panel's columns of the outer panel: the interchanges of the panels after it (one launch)
+        const int npan = (JB + NB - 1) / NB;
+        if (npan > 1 && (rc = laswp(K0 + NB, JB - NB, K0, K0 + NB, 0, 0, NB, npan - 1, H))) return rc;
         M25_CHECK(cudaEventRecord(ev_panel, H));                          // block k's L and pivots are final
         if (KE < n) {                                                       // H: the next block's columns
             if (next_pending) M25_CHECK(cudaStreamWaitEvent(H, ev_next, 0));
-            if ((rc = laswp(K0, JB, KE, KE2, H))) return rc;
-            for (int k0 = K0; k0 < KE; k0 += NB) {                          // U12 = L11^-1 A12 by blocks of NB
-                const int jb = std::min(NB, KE - k0);
-                if ((rc = trsm(k0, jb, KE, KE2, H))) return rc;
-                if ((rc = gemm(k0 + jb, KE - k0 - jb, KE, KE2 - KE, k0, jb, true, H))) return rc;
-            }
+            if ((rc = trsm_outer(K0, JB, KE, KE2, H))) return rc;          // interchanges and U12 in one launch
             if ((rc = gemm(KE, n - KE, KE, KE2 - KE, K0, JB, true, H))) return rc;
         }
         M25_CHECK(cudaStreamWaitEvent(Lo, ev_panel, 0));                    // Lo: the left and the far columns
-        if ((rc = laswp(K0, JB, 0, K0, Lo))) return rc;
+        if ((rc = laswp(K0, JB, 0, K0, KE2, n, 0, 1, Lo))) return rc;      // (one launch for both)
         next_pending = false;
         if (KE2 < n) {
-            if ((rc = laswp(K0, JB, KE2, n, Lo))) return rc;
             for (int k0 = K0; k0 < KE; k0 += NB) {
                 const int jb = std::min(NB, KE - k0);
-                if ((rc = trsm(k0, jb, KE2, n, Lo))) return rc;
+                if ((rc = trsm(k0, jb, KE2, n, false, Lo))) return rc;
                 if ((rc = gemm(k0 + jb, KE - k0 - jb, KE2, n - KE2, k0, jb, true, Lo))) return rc;
             }
             if ((rc = gemm(KE, n - KE, KE2, KE3 - KE2, K0, JB, true, Lo))) return rc;   // block k + 2's columns

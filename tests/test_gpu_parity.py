@@ -244,6 +244,38 @@ def test_lu_matches_lapack(single, n):
     assert np.abs(Rd.cpu().numpy() - x).max() < (1e-4 if single else 1e-11) * np.abs(x).max()
 
 
+@pytest.mark.parametrize('pattern', ['shift', 'reverse', 'random'])
+@pytest.mark.parametrize('single,tf32', [(0, 0), (1, 0), (1, 1)])
+def test_lu_row_interchange_patterns(pattern, single, tf32):
+    """Row interchanges composed into one permutation per panel (the LU's interchange plans): matrices whose
+    pivots are forced (Z^T = s P + noise, P a permutation: column j's pivot is the row P puts there), against
+    LAPACK's pivots and factor. 'shift' (p_i = i + 1) makes every interchange chain to the one before it (the
+    longest chains the plan resolves); 'reverse' moves rows far below the panel; N = 700: three outer panels, the
+    last ragged, so the in-panel, look-ahead and far-column interchanges all run."""
+    from mom25d_b200 import _lib
+    n = 700
+    rng = np.random.default_rng(7)
+    sigma = {'shift': (np.arange(n) + 1) % n, 'reverse': np.arange(n)[::-1].copy(),
+             'random': rng.permutation(n)}[pattern]
+    dt = np.complex64 if single else np.complex128
+    A = 0.1 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    A[sigma, np.arange(n)] += 10 * n * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
+    Z = np.ascontiguousarray(A.T).astype(dt)
+    Zd = _lib.dev(Z)
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(_lib.lib().m25_getrf_workspace(n, single))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    _lib.check(_lib.lib().m25_getrf(_lib.P(Zd), ctypes.c_long(n), n, _lib.P(ipiv), single, tf32, _lib.P(work),
+                                    ctypes.c_size_t(nb), _lib.stream_ptr()))
+    _lib.sync_check()
+    lu_ref, piv_ref = sla.lu_factor(Z.T.astype(complex))
+    assert np.count_nonzero(piv_ref != np.arange(n)) > n // 3
+    assert np.array_equal(ipiv.cpu().numpy(), piv_ref)
+    lu = Zd.cpu().numpy().T
+    tol = 1e-5 if single else 1e-13
+    assert np.abs(lu - lu_ref).max() < tol * np.abs(lu_ref).max()
+
+
 def test_complex_bessel_matches_the_reference(golden):
     from mom25d_b200 import _lib
     z = _lib.dev(golden['jn_z'], np.complex128)
