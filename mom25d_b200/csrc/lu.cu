@@ -95,12 +95,28 @@ __device__ __forceinline__ void warp_argmax(R &v, int &row)
 // The panel (GEPP over jb <= NB columns k0 .., rows k0 .. n) with each block's rows in shared memory for the whole
 // panel (Ps[c * cs + i] is row r0 + i, column k0 + c): global memory is read once and written once. Per column j:
 // (1) the block's candidate; (2) warp 0 brings the candidate row and the diagonal row (where the block holds it) up
-// to date and publishes them with the candidate; (3) the rest of the previous column's rank-1 update (columns
-// j + 1 ..), deferred to here so that it runs while the exchange is in flight; (4) every block's candidate read and
-// reduced; (5) the pivot row and the diagonal row (from the block's own shared memory where it holds them);
-// (6) the interchange, the scaling of column j and the update of column j + 1 only, which yields the next
-// candidates. Two round trips to L2 and three block barriers a column; the arithmetic of every entry is that of
-// the unpipelined order (a -= l U, once per column, in column order).
+// to date and publishes them with the candidate; (3) the deferred part of the update (below), run while the
+// exchange is in flight; (4) every block's candidate read and reduced; (5) the pivot row and the diagonal row (from
+// the block's own shared memory where it holds them); (6) the interchange, the scaling of column j and the update
+// of column j + 1 only, which yields the next candidates. Two round trips to L2 and three block barriers a column.
+//
+// The updates are grouped by GRP columns so that the columns past the current group are read and written once a
+// group rather than once a column (the rank-1 updates made the panel bound by shared-memory bandwidth): within the
+// group [g0, gend) a column's update reaches only the group's own later columns; at the next group's first column,
+// step (3) applies the whole group's GRP terms to every column past it (and step 6 of the group's last column to
+// the column after it, which is searched next). A row published as a candidate goes out in full (the group's terms
+// due on the columns past the group added on the way, not stored), the diagonal row as stored (it moves into
+// another block's rows, where those terms are still applied). Every entry still takes its terms a -= l U one at a
+// time in column order: the results are those of the column-by-column order.
+#define GRP 8
+// the block's candidate from the warps' ones (sv, si of nw warps): one butterfly in every warp
+template <typename R>
+__device__ __forceinline__ void block_argmax(R &v, int &row, const R *sv, const int *si, int lane, int nw)
+{
+    v = lane < nw ? sv[lane] : (R)-1;
+    row = lane < nw ? si[lane] : PANEL_NONE;
+    warp_argmax(v, row);
+}
 template <typename R>
 __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, int n, int k0, int jb, int *ipiv,
                                                               PanelWork pw, int *err)
@@ -118,7 +134,8 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
     const int r0 = k0 + b * cs, r1 = min(n, r0 + cs);
     const int nr = max(0, r1 - r0);
     const int PW = jb * WPC;                              // payload words of one panel row
-    __shared__ __align__(16) C U[NB], D[NB];
+    __shared__ __align__(16) C U[NB], D[NB], W[NB];       // pivot row, diagonal row, this block's published row
+    __shared__ __align__(16) C Ug[GRP][NB];               // the current group's pivot rows
     __shared__ R sv[NWARP], sv2[NWARP];
     __shared__ int si[NWARP], si2[NWARP], sw2[NWARP];
     __shared__ int s_fail;
@@ -138,26 +155,40 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         const int col = k0 + j, par = j & 1;
         const unsigned flag = (unsigned)col + 1u;
         const bool own_col = col >= r0 && col < r1;
+        const int g0 = j - j % GRP, gend = min(g0 + GRP, jb);
+        const bool gstart = j > 0 && j == g0;             // the previous group's terms are due past column j
+        const int pg0 = g0 - GRP;
         // (1) the block's candidate
         warp_argmax(best, bi);
         if (lane == 0) { sv[wid] = best; si[wid] = bi; }
         __syncthreads();                                  // (column j is complete for every row >= col)
-        best = sv[0]; bi = si[0];
-        for (int w = 1; w < NWARP; ++w)
-            if (sv[w] > best || (sv[w] == best && si[w] < bi)) { best = sv[w]; bi = si[w]; }
+        block_argmax(best, bi, sv, si, lane, NWARP);
         const int ec = own_col ? col - r0 : -1;                          // rows brought up to date eagerly
         const int eb = (bi != PANEL_NONE && bi != col) ? bi - r0 : -1;
-        // (2) warp 0: the previous column's update of columns j + 1 .. of those rows, then the block's record
+        const int ep = bi != PANEL_NONE ? bi - r0 : -1;                  // the candidate's row (ec if bi == col)
+        // (2) warp 0: the deferred update of those rows (as step 3 does it for the others), then the block's record
         if (wid == 0) {
             if (j > 0) {
                 for (int q = 0; q < 2; ++q) {
                     const int e = q ? eb : ec;
                     if (e < 0) continue;
-                    const C lp = Ps[(j - 1) * cs + e];
-                    for (int c = j + 1 + lane; c < jb; c += 32) {
-                        C a = Ps[c * cs + e];
-                        cfms<R>(a, lp, U[c]);
-                        Ps[c * cs + e] = a;
+                    if (gstart) {
+                        C lr[GRP];
+#pragma unroll
+                        for (int s = 0; s < GRP; ++s) lr[s] = Ps[(pg0 + s) * cs + e];
+                        for (int c = j + 1 + lane; c < jb; c += 32) {
+                            C a = Ps[c * cs + e];
+#pragma unroll
+                            for (int s = 0; s < GRP; ++s) cfms<R>(a, lr[s], Ug[s][c]);
+                            Ps[c * cs + e] = a;
+                        }
+                    } else {
+                        const C lp = Ps[(j - 1) * cs + e];
+                        for (int c = j + 1 + lane; c < gend; c += 32) {
+                            C a = Ps[c * cs + e];
+                            cfms<R>(a, lp, U[c]);
+                            Ps[c * cs + e] = a;
+                        }
                     }
                 }
                 __syncwarp();
@@ -169,32 +200,52 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                 for (int q = 0; q < VW; ++q) ll_put(rec + q, bv32[q], flag);
                 ll_put(rec + VW, (unsigned)bi, flag);
             }
-            for (int t = lane; t < PW; t += 32) {
-                const int c = t / WPC, q = t % WPC;
-                if (bi != PANEL_NONE)
-                    ll_put(pw.ll_row + ((size_t)par * G + b) * (4 * NB) + t,
-                           P32[((size_t)c * cs + (bi - r0)) * WPC + q], flag);
-                if (own_col)
-                    ll_put(pw.ll_drow + (size_t)par * (4 * NB) + t, P32[((size_t)c * cs + (col - r0)) * WPC + q], flag);
+            unsigned long long *rrow = pw.ll_row + ((size_t)par * G + b) * (4 * NB);
+            unsigned long long *drow = pw.ll_drow + (size_t)par * (4 * NB);
+            for (int c = lane; c < jb; c += 32) {
+                if (ep >= 0) {                             // the candidate row in full
+                    C a = Ps[c * cs + ep];
+                    if (c >= gend)
+                        for (int s = g0; s < j; ++s) cfms<R>(a, Ps[s * cs + ep], Ug[s - g0][c]);
+                    W[c] = a;
+                    const unsigned *a32 = reinterpret_cast<const unsigned *>(&a);
+#pragma unroll
+                    for (int q = 0; q < WPC; ++q) ll_put(rrow + c * WPC + q, a32[q], flag);
+                }
+                if (own_col) {                             // the diagonal row as stored
+                    const C d = Ps[c * cs + ec];
+                    const unsigned *d32 = reinterpret_cast<const unsigned *>(&d);
+#pragma unroll
+                    for (int q = 0; q < WPC; ++q) ll_put(drow + c * WPC + q, d32[q], flag);
+                }
             }
+            __syncwarp();
         }
-        // (3) the previous column's update of columns j + 1 .. for the other rows >= col: two threads a row
-        // (adjacent lanes), columns j + 1 + sub, j + 3 + sub, ..., four at a time with their loads issued together
-        if (j > 0) {
+        // (3) the deferred update for the other rows >= col
+        if (gstart) {
+            // the previous group's GRP terms on every column past j: a thread a row (a warp on consecutive rows),
+            // its multipliers in registers, the group's pivot rows read as broadcasts
+            for (int i = max(0, col - r0) + tid; i < nr; i += PANEL_THREADS) {
+                if (i == ec || i == eb) continue;
+                C lr[GRP];
+#pragma unroll
+                for (int s = 0; s < GRP; ++s) lr[s] = Ps[(pg0 + s) * cs + i];
+#pragma unroll 2
+                for (int c = j + 1; c < jb; ++c) {
+                    C a = Ps[c * cs + i];
+#pragma unroll
+                    for (int s = 0; s < GRP; ++s) cfms<R>(a, lr[s], Ug[s][c]);
+                    Ps[c * cs + i] = a;
+                }
+            }
+        } else if (j > 0) {
+            // the previous column's term on the group's columns past j: two threads a row (adjacent lanes),
+            // columns j + 1 + sub, j + 3 + sub, ...
             const int sub = tid & 1;
             for (int i = max(0, col - r0) + (tid >> 1); i < nr; i += PANEL_THREADS / 2) {
                 if (i == ec || i == eb) continue;
                 const C lp = Ps[(j - 1) * cs + i];
-                int c = j + 1 + sub;
-                for (; c + 6 < jb; c += 8) {
-                    C a0 = Ps[c * cs + i], a1 = Ps[(c + 2) * cs + i], a2 = Ps[(c + 4) * cs + i],
-                      a3 = Ps[(c + 6) * cs + i];
-                    const C u0 = U[c], u1 = U[c + 2], u2 = U[c + 4], u3 = U[c + 6];
-                    cfms<R>(a0, lp, u0); cfms<R>(a1, lp, u1); cfms<R>(a2, lp, u2); cfms<R>(a3, lp, u3);
-                    Ps[c * cs + i] = a0; Ps[(c + 2) * cs + i] = a1;
-                    Ps[(c + 4) * cs + i] = a2; Ps[(c + 6) * cs + i] = a3;
-                }
-                for (; c < jb; c += 2) {
+                for (int c = j + 1 + sub; c < gend; c += 2) {
                     C a = Ps[c * cs + i];
                     cfms<R>(a, lp, U[c]);
                     Ps[c * cs + i] = a;
@@ -223,22 +274,28 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         if (lane == 0) { sv2[wid] = bv; si2[wid] = brow; sw2[wid] = bw; }
         __syncthreads();                                  // (and the deferred update is complete)
         if (s_fail) return;
-        bv = sv2[0]; brow = si2[0]; bw = sw2[0];
-        for (int w = 1; w < NWARP; ++w)
-            if (sv2[w] > bv || (sv2[w] == bv && si2[w] < brow)) { bv = sv2[w]; brow = si2[w]; bw = sw2[w]; }
+        bv = lane < NWARP ? sv2[lane] : (R)-1;              // the block's reduction by one butterfly a warp
+        brow = lane < NWARP ? si2[lane] : PANEL_NONE;
+        bw = lane < NWARP ? sw2[lane] : -1;
+        for (int o = 16; o; o >>= 1) {
+            const R ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, brow, o), ow = __shfl_xor_sync(0xffffffffu, bw, o);
+            if (ov > bv || (ov == bv && orow < brow)) { bv = ov; brow = orow; bw = ow; }
+        }
         if (bw < 0 || bw >= G) { if (tid == 0) dev_error(err, M25_DEV_INDEX); return; }
         const int p = brow;
         if (b == 0 && tid == 0) ipiv[col] = p;
-        // (5) every block: U[j ..]; the block that holds row col: all of U; the block that holds row p: D. A row
-        // the block holds comes from its own shared memory: at most one read from L2 a word
+        // (5) every block: U[j ..]; the block that holds row col: all of U; the block that holds row p: D. The
+        // pivot row comes in full (from W where the block published it), the diagonal row as stored. U also goes
+        // into the group's rows for the terms past the group
         if (tid < PW) {
-            const int c = tid / WPC, q = tid % WPC;
+            const int q = tid % WPC;
             const bool own_p = b == bw, need_u = own_col || tid >= j * WPC;
             unsigned u = 0, d = 0;
             bool ok = true;
             if (own_p) {
-                u = P32[((size_t)c * cs + (p - r0)) * WPC + q];
-                if (own_col) d = P32[((size_t)c * cs + (col - r0)) * WPC + q];
+                u = reinterpret_cast<const unsigned *>(W)[tid];
+                if (own_col) d = P32[((size_t)(tid / WPC) * cs + (col - r0)) * WPC + q];
                 else ok = ll_wait<1>(pw.ll_drow + (size_t)par * (4 * NB) + tid, 0, flag, &d, err);
             } else if (need_u) {
                 ok = ll_wait<1>(pw.ll_row + ((size_t)par * G + bw) * (4 * NB) + tid, 0, flag, &u, err);
@@ -247,7 +304,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                 s_fail = 1;
                 dev_error(err, M25_DEV_TIMEOUT);
             } else {
-                if (own_p || need_u) reinterpret_cast<unsigned *>(U)[tid] = u;
+                if (own_p || need_u) {
+                    reinterpret_cast<unsigned *>(U)[tid] = u;
+                    reinterpret_cast<unsigned *>(Ug[j - g0])[tid] = u;
+                }
                 if (own_p) reinterpret_cast<unsigned *>(D)[tid] = d;
             }
         }
@@ -272,6 +332,8 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                 if (half == 1 && b == bw && p != col && e != j && e != j + 1) Ps[e * cs + (p - r0)] = D[e];
             }
         }
+        // column j + 1: the group's last term here, or (the group's last column) every term of the group
+        const bool gfin = j + 1 == gend && j + 1 < jb;
         best = -1; bi = PANEL_NONE;
         for (int i = max(0, col - r0) + tid; i < nr; i += PANEL_THREADS) {
             const int row = r0 + i;
@@ -281,6 +343,8 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
             Ps[j * cs + i] = l;
             if (j + 1 < jb) {
                 C a = isp ? D[j + 1] : Ps[(j + 1) * cs + i];
+                if (gfin)
+                    for (int s = g0; s < j; ++s) cfms<R>(a, isp ? D[s] : Ps[s * cs + i], Ug[s - g0][j + 1]);
                 cfms<R>(a, l, U[j + 1]);
                 Ps[(j + 1) * cs + i] = a;
                 const R v = abs1(a);
@@ -1623,7 +1687,9 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     int smem_optin = 0, dev = 0;
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const int smem_cap = smem_optin - 4096;                          // (the kernel's static shared memory)
+    cudaFuncAttributes pfa;
+    M25_CHECK(cudaFuncGetAttributes(&pfa, k_panel_smem<R>));
+    const int smem_cap = smem_optin - (int)pfa.sharedSizeBytes;      // less the kernel's static shared memory
     M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
     // Blocks of the panel: few enough that the cooperative launch finds its SMs quickly while the other stream's
     // update holds the rest (the exchange costs about the same from 37 to 148 blocks), but at least as many as
