@@ -78,8 +78,53 @@ __device__ __forceinline__ bool ll_wait(const unsigned long long *p, int stride,
 }
 
 
+// The same exchange inside a thread-block cluster: each block's records in its own shared memory, written there and
+// read by the other blocks of the cluster through distributed shared memory (generic addresses of their shared
+// memory), at cluster scope; polled the same bounded way.
+__device__ __forceinline__ void cl_put(unsigned long long *p, unsigned payload, unsigned flag)
+{
+    const unsigned long long w = ((unsigned long long)flag << 32) | payload;
+    asm volatile("st.relaxed.cluster.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ unsigned long long cl_get(const unsigned long long *p)
+{
+    unsigned long long w;
+    asm volatile("ld.relaxed.cluster.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+    return w;
+}
+template <bool CL>
+__device__ __forceinline__ void x_put(unsigned long long *p, unsigned payload, unsigned flag)
+{
+    if (CL) cl_put(p, payload, flag);
+    else ll_put(p, payload, flag);
+}
+template <int K, bool CL>
+__device__ __forceinline__ bool x_wait(const unsigned long long *p, int stride, unsigned flag, unsigned *out,
+                                       const int *err)
+{
+    if (!CL) return ll_wait<K>(p, stride, flag, out, err);
+    long it = 0;
+    for (;;) {
+        bool all = true;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const unsigned long long w = cl_get(p + (size_t)q * stride);
+            out[q] = (unsigned)w;
+            all = all && (unsigned)(w >> 32) == flag;
+        }
+        if (all) return true;
+        if ((++it & 1023) == 0 && (it > (1L << 22) || *(volatile const int *)err)) return false;
+    }
+}
+
 #define PANEL_NONE 0x7fffffff
 #define LL_REC 32             // words a candidate record (256 bytes: polled by every block, one record a line pair)
+// a cluster panel's records, after its rows in shared memory
+struct PanelRecords {
+    unsigned long long cand[2][LL_REC];
+    unsigned long long row[2][4 * NB];
+    unsigned long long drow[2][4 * NB];
+};
 
 // The largest |re| + |im| and its row over a warp (the first row on ties: izamax / icamax)
 template <typename R>
@@ -108,6 +153,12 @@ __device__ __forceinline__ void warp_argmax(R &v, int &row)
 // due on the columns past the group added on the way, not stored), the diagonal row as stored (it moves into
 // another block's rows, where those terms are still applied). Every entry still takes its terms a -= l U one at a
 // time in column order: the results are those of the column-by-column order.
+//
+// CL: the panel's blocks are one thread-block cluster (a panel of up to 16 blocks' rows) and the exchange goes
+// through distributed shared memory instead of L2: the same records and bounded polls, each block's records after
+// its rows in its own shared memory (zeroed, then a cluster barrier, before the first column; a cluster barrier
+// before any block leaves, so that no block reads the shared memory of one that has). The other blocks' records
+// are a few hundred cycles away instead of an L2 round trip, which the trailing update's traffic makes long.
 #define GRP 8
 // the block's candidate from the warps' ones (sv, si of nw warps): one butterfly in every warp
 template <typename R>
@@ -117,7 +168,7 @@ __device__ __forceinline__ void block_argmax(R &v, int &row, const R *sv, const 
     row = lane < nw ? si[lane] : PANEL_NONE;
     warp_argmax(v, row);
 }
-template <typename R>
+template <typename R, bool CL>
 __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, int n, int k0, int jb, int *ipiv,
                                                               PanelWork pw, int *err)
 {
@@ -134,6 +185,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
     const int r0 = k0 + b * cs, r1 = min(n, r0 + cs);
     const int nr = max(0, r1 - r0);
     const int PW = jb * WPC;                              // payload words of one panel row
+    PanelRecords *RX = reinterpret_cast<PanelRecords *>(panel_raw + ((size_t)cs * jb * sizeof(C) + 15) / 16 * 16);
     __shared__ __align__(16) C U[NB], D[NB], W[NB];       // pivot row, diagonal row, this block's published row
     __shared__ __align__(16) C Ug[GRP][NB];               // the current group's pivot rows
     __shared__ R sv[NWARP], sv2[NWARP];
@@ -144,6 +196,12 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         Ps[c * cs + i] = ldc<R>(A, (size_t)(k0 + c) * lda + r0 + i);
     }
     if (tid == 0) s_fail = 0;
+    if constexpr (CL) {
+        unsigned long long *rz = reinterpret_cast<unsigned long long *>(RX);
+        for (int e = tid; e < (int)(sizeof(PanelRecords) / 8); e += PANEL_THREADS) rz[e] = 0ull;
+        __syncthreads();
+        cooperative_groups::this_cluster().sync();
+    }
     __syncthreads();
     R best = -1;                                          // this thread's candidate for column 0
     int bi = PANEL_NONE;
@@ -155,6 +213,24 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         const int col = k0 + j, par = j & 1;
         const unsigned flag = (unsigned)col + 1u;
         const bool own_col = col >= r0 && col < r1;
+        // this column's records: where this block publishes, and where block q's are read
+        unsigned long long *my_rec, *my_row, *my_drow;
+        if constexpr (CL) {
+            my_rec = RX->cand[par]; my_row = RX->row[par]; my_drow = RX->drow[par];
+        } else {
+            my_rec = pw.ll_cand + ((size_t)par * G + b) * LL_REC;
+            my_row = pw.ll_row + ((size_t)par * G + b) * (4 * NB);
+            my_drow = pw.ll_drow + (size_t)par * (4 * NB);
+        }
+        auto rec_of = [&](int q, int which) -> const unsigned long long * {   // which: 0 record, 1 row, 2 diagonal
+            if constexpr (CL) {
+                unsigned long long *mine = which == 0 ? RX->cand[par] : which == 1 ? RX->row[par] : RX->drow[par];
+                return cooperative_groups::this_cluster().map_shared_rank(mine, (unsigned)q);
+            } else {
+                return which == 0 ? pw.ll_cand + ((size_t)par * G + q) * LL_REC
+                     : which == 1 ? pw.ll_row + ((size_t)par * G + q) * (4 * NB) : pw.ll_drow + (size_t)par * (4 * NB);
+            }
+        };
         const int g0 = j - j % GRP, gend = min(g0 + GRP, jb);
         const bool gstart = j > 0 && j == g0;             // the previous group's terms are due past column j
         const int pg0 = g0 - GRP;
@@ -193,15 +269,15 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                 }
                 __syncwarp();
             }
-            unsigned long long *rec = pw.ll_cand + ((size_t)par * G + b) * LL_REC;
+            unsigned long long *rec = my_rec;
             if (lane == 0) {
                 const unsigned *bv32 = reinterpret_cast<const unsigned *>(&best);
 #pragma unroll
-                for (int q = 0; q < VW; ++q) ll_put(rec + q, bv32[q], flag);
-                ll_put(rec + VW, (unsigned)bi, flag);
+                for (int q = 0; q < VW; ++q) x_put<CL>(rec + q, bv32[q], flag);
+                x_put<CL>(rec + VW, (unsigned)bi, flag);
             }
-            unsigned long long *rrow = pw.ll_row + ((size_t)par * G + b) * (4 * NB);
-            unsigned long long *drow = pw.ll_drow + (size_t)par * (4 * NB);
+            unsigned long long *rrow = my_row;
+            unsigned long long *drow = my_drow;
             for (int c = lane; c < jb; c += 32) {
                 if (ep >= 0) {                             // the candidate row in full
                     C a = Ps[c * cs + ep];
@@ -210,13 +286,13 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
                     W[c] = a;
                     const unsigned *a32 = reinterpret_cast<const unsigned *>(&a);
 #pragma unroll
-                    for (int q = 0; q < WPC; ++q) ll_put(rrow + c * WPC + q, a32[q], flag);
+                    for (int q = 0; q < WPC; ++q) x_put<CL>(rrow + c * WPC + q, a32[q], flag);
                 }
                 if (own_col) {                             // the diagonal row as stored
                     const C d = Ps[c * cs + ec];
                     const unsigned *d32 = reinterpret_cast<const unsigned *>(&d);
 #pragma unroll
-                    for (int q = 0; q < WPC; ++q) ll_put(drow + c * WPC + q, d32[q], flag);
+                    for (int q = 0; q < WPC; ++q) x_put<CL>(drow + c * WPC + q, d32[q], flag);
                 }
             }
             __syncwarp();
@@ -257,7 +333,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         int brow = PANEL_NONE, bw = -1;
         if (tid < G) {
             unsigned wv[VW + 1];
-            if (!ll_wait<VW + 1>(pw.ll_cand + ((size_t)par * G + tid) * LL_REC, 1, flag, wv, err)) {
+            if (!x_wait<VW + 1, CL>(rec_of(tid, 0), 1, flag, wv, err)) {
                 s_fail = 1;
                 dev_error(err, M25_DEV_TIMEOUT);
             } else if ((int)wv[VW] != PANEL_NONE) {
@@ -273,7 +349,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         }
         if (lane == 0) { sv2[wid] = bv; si2[wid] = brow; sw2[wid] = bw; }
         __syncthreads();                                  // (and the deferred update is complete)
-        if (s_fail) return;
+        if (s_fail) goto finish;
         bv = lane < NWARP ? sv2[lane] : (R)-1;              // the block's reduction by one butterfly a warp
         brow = lane < NWARP ? si2[lane] : PANEL_NONE;
         bw = lane < NWARP ? sw2[lane] : -1;
@@ -282,7 +358,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
             const int orow = __shfl_xor_sync(0xffffffffu, brow, o), ow = __shfl_xor_sync(0xffffffffu, bw, o);
             if (ov > bv || (ov == bv && orow < brow)) { bv = ov; brow = orow; bw = ow; }
         }
-        if (bw < 0 || bw >= G) { if (tid == 0) dev_error(err, M25_DEV_INDEX); return; }
+        if (bw < 0 || bw >= G) {
+            if (tid == 0) dev_error(err, M25_DEV_INDEX);
+            goto finish;
+        }
         const int p = brow;
         if (b == 0 && tid == 0) ipiv[col] = p;
         // (5) every block: U[j ..]; the block that holds row col: all of U; the block that holds row p: D. The
@@ -296,9 +375,9 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
             if (own_p) {
                 u = reinterpret_cast<const unsigned *>(W)[tid];
                 if (own_col) d = P32[((size_t)(tid / WPC) * cs + (col - r0)) * WPC + q];
-                else ok = ll_wait<1>(pw.ll_drow + (size_t)par * (4 * NB) + tid, 0, flag, &d, err);
+                else ok = x_wait<1, CL>(rec_of((col - k0) / cs, 2) + tid, 0, flag, &d, err);
             } else if (need_u) {
-                ok = ll_wait<1>(pw.ll_row + ((size_t)par * G + bw) * (4 * NB) + tid, 0, flag, &u, err);
+                ok = x_wait<1, CL>(rec_of(bw, 1) + tid, 0, flag, &u, err);
             }
             if (!ok) {
                 s_fail = 1;
@@ -312,7 +391,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
             }
         }
         __syncthreads();
-        if (s_fail) return;
+        if (s_fail) goto finish;
         // (6) rows col and p interchanged (whole panel rows), column j scaled by 1 / pivot, column j + 1 updated
         // (the rest of this column's update is deferred to the next column's step 3); the next candidates
         const C piv = U[j];
@@ -357,6 +436,8 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_panel_smem(R *A, long lda, in
         int c = e / nr, i = e % nr;
         stc<R>(A, (size_t)(k0 + c) * lda + r0 + i, Ps[c * cs + i]);
     }
+finish:
+    if constexpr (CL) cooperative_groups::this_cluster().sync();   // (no block leaves while another may read it)
 }
 
 // The same with the rows in global memory (when a block's rows do not fit in shared memory).
@@ -1688,9 +1769,38 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes pfa;
-    M25_CHECK(cudaFuncGetAttributes(&pfa, k_panel_smem<R>));
+    M25_CHECK(cudaFuncGetAttributes(&pfa, k_panel_smem<R, false>));
     const int smem_cap = smem_optin - (int)pfa.sharedSizeBytes;      // less the kernel's static shared memory
-    M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+    M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cap));
+    // The cluster panel (the exchange in distributed shared memory) takes the panels whose rows fit a cluster's
+    // blocks: as many blocks as the largest cluster this kernel can have on the device (16 where non-portable
+    // sizes are allowed), a block's rows and its records in its shared memory. M25_PANEL_CLUSTER=0: never.
+    int cl_max = 0, cl_rows_cap = 0;
+    {
+        const char *e = getenv("M25_PANEL_CLUSTER");
+        if (!e || atoi(e) != 0) {
+            cudaFuncAttributes cfa;
+            M25_CHECK(cudaFuncGetAttributes(&cfa, k_panel_smem<R, true>));
+            const int cl_smem = smem_optin - (int)cfa.sharedSizeBytes;
+            M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, cl_smem));
+            M25_CHECK(cudaFuncSetAttribute(k_panel_smem<R, true>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cl_rows_cap = (int)(((size_t)cl_smem - sizeof(PanelRecords) - 16) / (sizeof(cpx<R>) * NB));
+            cudaLaunchConfig_t qc = {};
+            cudaLaunchAttribute qa[1];
+            qa[0].id = cudaLaunchAttributeClusterDimension;
+            qa[0].val.clusterDim.x = 16; qa[0].val.clusterDim.y = 1; qa[0].val.clusterDim.z = 1;
+            qc.gridDim = dim3(16); qc.blockDim = dim3(PANEL_THREADS); qc.dynamicSmemBytes = (size_t)cl_smem;
+            qc.attrs = qa; qc.numAttrs = 1;
+            int mc = 0;
+            if (cudaOccupancyMaxPotentialClusterSize(&mc, (void *)k_panel_smem<R, true>, &qc) != cudaSuccess) {
+                (void)cudaGetLastError();
+                mc = 0;
+            }
+            cl_max = std::min(16, mc);
+            if (const char *m = getenv("M25_PANEL_CLUSTER_MAX")) cl_max = std::min(cl_max, atoi(m));
+            if (cl_max < 2) cl_max = 0;
+        }
+    }
     // Blocks of the panel: few enough that the cooperative launch finds its SMs quickly while the other stream's
     // update holds the rest (the exchange costs about the same from 37 to 148 blocks), but at least as many as
     // the panel's rows need to fit in shared memory (M25_PANEL_BLOCKS: tuning)
@@ -1786,9 +1896,21 @@ static int getrf_impl(R *A, long lda, int n, int *ipiv, int tf32, void *work, si
             const int cs = (n - k0 + Gp - 1) / Gp;
             const size_t psmem = sizeof(cpx<R>) * (size_t)cs * jb;
             void *args[] = {&A, &lda, &n, (void *)&k0, (void *)&jb, &ipiv, &pw, &err};
-            if (psmem <= (size_t)smem_cap) {                           // (flagged records: no barrier to reset)
-                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R>, dim3(Gp), dim3(PANEL_THREADS), args,
-                                                      psmem, H));
+            const int rows = n - k0;
+            if (cl_max && rows <= cl_max * cl_rows_cap) {               // one cluster, at least 64 rows a block
+                const int Gc = std::min(cl_max, std::max(2, (rows + 63) / 64));
+                const int csc = (rows + Gc - 1) / Gc;
+                cudaLaunchConfig_t lc = {};
+                cudaLaunchAttribute la1[1];
+                la1[0].id = cudaLaunchAttributeClusterDimension;
+                la1[0].val.clusterDim.x = (unsigned)Gc; la1[0].val.clusterDim.y = 1; la1[0].val.clusterDim.z = 1;
+                lc.gridDim = dim3(Gc); lc.blockDim = dim3(PANEL_THREADS);
+                lc.dynamicSmemBytes = ((size_t)csc * jb * sizeof(cpx<R>) + 15) / 16 * 16 + sizeof(PanelRecords);
+                lc.stream = H; lc.attrs = la1; lc.numAttrs = 1;
+                M25_CHECK(cudaLaunchKernelExC(&lc, (const void *)k_panel_smem<R, true>, args));
+            } else if (psmem <= (size_t)smem_cap) {                    // (flagged records: no barrier to reset)
+                M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel_smem<R, false>, dim3(Gp), dim3(PANEL_THREADS),
+                                                      args, psmem, H));
             } else {
                 M25_CHECK(cudaMemsetAsync(bar, 0, (2 + 2 * (size_t)G) * sizeof(unsigned), H));
                 M25_CHECK(cudaLaunchCooperativeKernel((void *)k_panel<R>, dim3(Gp), dim3(PANEL_THREADS), args, 0, H));
