@@ -219,8 +219,7 @@ def run_gpu(args, rank, world):
 
     def cold():
         """A sweep starts with no kept LUs and nothing learnt (the warm-up leaves some)."""
-        ds.kept, ds.reach, ds.t_iter, ds.mixed_failed = [], float(np.log(2.0)), None, 0.0
-        ds.kept64, ds.t_iter64 = None, None
+        ds.forget()
 
     for i in range(args.warmup):
         step_device(mine[i % len(mine)], 'mixed')
@@ -328,6 +327,7 @@ def run_gpu(args, rank, world):
                      "backward_error": [float('%.3g' % x) for x in berr]},
         "lu_ms": round(1000 * lu_avg, 3) if lu_ms else None, "factorisations": len(lu_ms), "paths": paths,
         "reuse_attempts": {"tried": len(attempts), "converged": sum(1 for a in attempts if a['ok'])},
+        "kept_lus_max": int(ds._keep_max()),
         "phases_ms_per_step": phases,
         "e2e": {"value": round(e2e, 4), "unit": "freq-solves/s", "h2d_bytes_per_step": bytes_h2d,
                 "d2h_bytes_per_step": bytes_d2h},

@@ -178,7 +178,7 @@ def run(board, freqs, slots=6, fp64_count=None, sequential_mixed=True):
         simm = Simulation.from_board(board, precision='mixed')
         simm.sparams(freqs[len(freqs) // 2])              # warm-up, then a cold sweep
         ds = simm.fast
-        ds.kept, ds.reach, ds.t_iter, ds.mixed_failed = [], float(np.log(2.0)), None, 0.0
+        ds.forget()
         S_m, wall_m = sequential_sweep(simm, freqs)
         out['sequential_mixed'] = dict(solves_per_s=round(len(freqs) / wall_m, 3), wall_s=round(wall_m, 3))
         out['max_dS_sequential_mixed_vs_fp64'] = max_dS([S_m[i] for i in isel], S_d)

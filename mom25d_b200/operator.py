@@ -8,7 +8,7 @@ FastOperator.solve_direct (mom25d fast.py:704-850) behind the same call, solve_d
   precision='mixed'   where the device holds a double Z and complex64 copies (24 N^2 bytes, the reference's hybrid
                       path, fast.py:996-1084 _solve_kept): Z filled in double and equilibrated; GMRES with the dense
                       double Z (one HBM-bound product a step) preconditioned by a complex64 LU kept from a nearby
-                      frequency (up to REUSE_KEEP of them, reach learnt as the reference does), else by a fresh
+                      frequency (up to KEEP_HBM of them, reach learnt as the reference does), else by a fresh
                       complex64 LU of Z's copy (trailing updates 3xTF32 on the tensor cores when tf32=True), kept;
                       where that does not converge, the double LU of the same Z (no second fill), and double up to
                       MIXED_RETRY x f.
@@ -37,7 +37,11 @@ MIXED_RTOL = 1e-6            # fast.py:366 (FastOperator.mixed_tol)
 PREDICT_AFTER = 6            # iterations after which a fresh factor's refinement may be given up as hopeless (gmres_batched)
 MIXED_RETRY = 1.25           # fast.py:252-254: after a mixed failure at f, double up to this x f
 REUSE_ITER = (8, 60)         # fast.py:260: the iterations a reused LU may take (its cap, from the cost of a fresh one)
-REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most
+REUSE_KEEP = 4               # fast.py:262: complex64 LUs kept at most (the reference's cap, set for host memory)
+KEEP_HBM = (16, 0.4)         # on the GPU: up to 16, in at most 40% of the device's memory (a complex64 LU of the
+                             # routed board, N = 18,788, is 2.8 GB). More kept factors leave a nearer one for each
+                             # frequency of a sweep: a reuse at 1.16x the kept frequency takes ~10 GMRES steps
+                             # (~100 ms) where a fresh factor takes ~215 ms (measured on the routed board)
 REUSE_GIVE_UP = (10, 0.05)   # a reused factor's GMRES ends from step 10 where a residual is still above 5% of |b| (a
                              # fresh LU follows). Rules that projected the rate of the last few steps to the cap were
                              # measured and dropped: GMRES plateaus and then speeds up, and they cut off attempts that
@@ -45,7 +49,13 @@ REUSE_GIVE_UP = (10, 0.05)   # a reused factor's GMRES ends from step 10 where a
 FRESH_STAGNATION = (10, 0.5)  # a fresh factor's GMRES ends at step 10 where a residual has not halved since step 1
                              # (measured on the routed board: at 0.5 GHz it stays at 2e-3 for all 30 steps; at 0.67 GHz
                              # it is 5x lower by step 10 and converges at 27)
-DOUBLE_REACH = float(np.log(1.5))  # |ln f / f0| within which the kept double factor preconditions a double solve
+DOUBLE_REACH = float(np.log(1.6))  # |ln f / f0| within which the kept double factor preconditions a double solve
+DOUBLE_UP = 1.6              # after a complex64 failure at f0, the frequencies up to this x f0 with the kept double factor
+                             # within reach go to it directly, past the reference's MIXED_RETRY: a complex64 factor is
+                             # as marginal there (its backward error times the condition of Z near 1: measured on the
+                             # routed board, a fresh complex64 LU at 0.67 and 0.78 GHz after 0.5 GHz failed converged or
+                             # stalled with rounding noise, a 990 ms step when it stalls) and the kept double factor
+                             # converges in ~5 GMRES steps
 
 
 SMALL = 1e-300
@@ -58,8 +68,11 @@ class SolveFailed(RuntimeError):
 class DirectSolver:
     """One board's device-resident direct solver (meshes, pairs, tables and factors stay on the GPU)."""
 
-    def __init__(self, geo, stream=None, tf32=False, log=None):
+    def __init__(self, geo, stream=None, tf32=False, log=None, keep=None):
+        """keep: complex64 LUs kept for reuse at most (None: KEEP_HBM, memory allowing; REUSE_KEEP is the
+        reference's own cap)."""
         self.geo, self.stream = geo, stream
+        self.keep = keep
         self.dg = DeviceGeometry(geo, stream)
         self.tf32 = tf32
         self.log = log if log is not None else []
@@ -67,7 +80,8 @@ class DirectSolver:
         self.iters = []
         self._work = {}
         self.kept = []                     # (f, factor record, dsc, seconds the fresh solve took): _solve_kept
-        self.reach = float(np.log(2.0))    # fast.py:862: |ln(f / f0)| within which a kept LU is tried
+        self.reach = float(np.log(2.0))    # fast.py:862: |ln(f / f0)| within which a kept LU is tried, at first
+        self.reach_log = []                # reuse attempts (f, |ln f / f0|, converged, iterations, cap): _reach_at
         self.t_iter = None
         self.mixed_failed = 0.0
         self.reuse = True
@@ -297,7 +311,9 @@ class DirectSolver:
         E = E.reshape(N, -1).contiguous()
         self.iters = []
         self.last_lu_ms = self.last_lu_c64_ms = None
-        if precision == 'mixed' and f <= MIXED_RETRY * self.mixed_failed:
+        near_double = (self.kept64 is not None and f <= DOUBLE_UP * self.mixed_failed and
+                       abs(np.log(f / self.kept64[0])) <= DOUBLE_REACH)
+        if precision == 'mixed' and (f <= MIXED_RETRY * self.mixed_failed or near_double):
             precision = 'double'                          # fast.py:740: near a failure, double
             if self._hybrid_fits():
                 return self._solve_double_near(f, E)
@@ -339,20 +355,44 @@ class DirectSolver:
         return 24.0 * N * N + 1e9 <= 0.8 * (free + held)
 
     def _keep_max(self):
-        """LUs that may stay resident (fast.py:959-960): REUSE_KEEP, memory allowing (8 N^2 bytes each)."""
+        """LUs that may stay resident (fast.py:959-960, memory allowing, 8 N^2 bytes each): the cap is keep, else
+        KEEP_HBM's count within its share of the device's memory."""
         if not self.reuse:
             return 0
         N = self.geo.N
-        free, _ = torch.cuda.mem_get_info()
+        free, total = torch.cuda.mem_get_info()
         kept = sum(k[1]['bytes'] for k in self.kept)
-        return int(min(REUSE_KEEP, (0.9 * (free + kept) - 0.4e9) // (8.0 * N * N)))
+        cap = self.keep if self.keep is not None else min(KEEP_HBM[0], int(KEEP_HBM[1] * total // (8.0 * N * N)))
+        return int(min(cap, (0.9 * (free + kept) - 0.4e9) // (8.0 * N * N)))
+
+    def forget(self):
+        """A new sweep: no kept factors, nothing learnt."""
+        self.kept, self.reach_log, self.t_iter, self.mixed_failed = [], [], None, 0.0
+        self.kept64, self.t_iter64 = None, None
+        self.reach = float(np.log(2.0))
 
     def _reusable(self, f):
-        """fast.py:974-980: the kept LU nearest in frequency, if within the reach."""
+        """fast.py:974-980: the kept LU nearest in frequency, if within the reach at f."""
         if not self.reuse or not self.kept:
             return None
         k = min(self.kept, key=lambda k: abs(np.log(f / k[0])))
-        return k if abs(np.log(f / k[0])) <= self.reach else None
+        return k if abs(np.log(f / k[0])) <= self._reach_at(f) else None
+
+    def _reach_at(self, f):
+        """The reach at f: the reference's rule (fast.py:989-994: a quick success widens it to 1.25 d, a failure
+        narrows it to 0.8 d) replayed over the attempts within an octave of f, in the order they were made. The
+        reference learns one reach for the whole band; how fast Z moves with f depends on where in the band f is
+        (measured on the routed board: reuses converge at 1.57x the kept frequency around 1-3 GHz and fail at
+        1.16x above 5 GHz), so a failure at 6 GHz no longer stops the reuses at 2 GHz."""
+        r = self.reach
+        for fa, d, ok, iters, cap in self.reach_log:
+            if abs(np.log(f / fa)) > np.log(2.0):
+                continue
+            if ok and iters <= cap // 2:
+                r = max(r, 1.25 * d)
+            elif not ok:
+                r = min(r, 0.8 * d)
+        return r
 
     def _drop_kept(self):
         """fast.py:982-987: drop the kept LU nearest another kept one."""
@@ -360,12 +400,9 @@ class DirectSolver:
         gap = [min((abs(lf[i] - y) for j, y in enumerate(lf) if j != i), default=0.0) for i in range(len(lf))]
         del self.kept[int(np.argmin(gap))]
 
-    def _reach_learn(self, d, ok, iters, cap):
-        """fast.py:989-994."""
-        if ok and max(iters) <= cap // 2:
-            self.reach = max(self.reach, 1.25 * d)
-        elif not ok:
-            self.reach = min(self.reach, 0.8 * d)
+    def _reach_learn(self, f, d, ok, iters, cap):
+        """fast.py:989-994: an attempt at f with a factor kept at |ln f / f0| = d, for _reach_at."""
+        self.reach_log.append((f, d, bool(ok), max(iters, default=0), cap))
 
     def _factor_c64(self, Z64):
         """A complex64 LU of its own (kept across frequencies): the factor in Z64's memory, pivots, the solves'
@@ -432,7 +469,7 @@ class DirectSolver:
             e0, t = self._mark(), time.perf_counter()
             Y, ok, rel = self.refine(A, B, M, cap, give_up=REUSE_GIVE_UP)
             self._learn_t_iter((time.perf_counter() - t) / max(1, max(self.iters, default=1)))
-            self._reach_learn(abs(np.log(f / f0)), ok, self.iters, cap)
+            self._reach_learn(f, abs(np.log(f / f0)), ok, self.iters, cap)
             self.attempts.append(dict(f=f, f0=f0, cap=cap, iters=max(self.iters, default=0), ok=ok, rel=rel))
             self._t('refine', e0)
             if ok:
