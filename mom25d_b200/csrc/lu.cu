@@ -1393,36 +1393,50 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// complex64: 128-row tiles and both inverses where a CTA owns two blocks; complex128 (16-byte entries): 32-row
+// tiles and one inverse buffer, so that a CTA of two blocks stays within shared memory
+template <typename R> constexpr int trsv_rt() { return sizeof(R) == 4 ? TRSV_RT : TRSV_RT / 4; }
+template <typename R> constexpr int trsv_nwmax() { return sizeof(R) == 4 ? 2 : 1; }
+template <typename R>
 static size_t trsv_pipe_smem(int per)
 {
-    typedef cpx<float> C;
-    const int nw = per <= 2 ? per : 1;
-    return sizeof(C) * (2 * (size_t)TRSV_RT * TRSV_TBP + (size_t)nw * TB * TRSV_TBP + TB * TRSV_YS +
+    typedef cpx<R> C;
+    const int nw = per <= trsv_nwmax<R>() ? per : 1;
+    return sizeof(C) * (2 * (size_t)trsv_rt<R>() * TRSV_TBP + (size_t)nw * TB * TRSV_TBP + TB * TRSV_YS +
                         (size_t)per * TB * TRSV_TS);
 }
 
 // out[r][c] (-)= sum_{k < kdim} M[r][k] X[k][c] for r < nrows (<= NT / TPR), c < KR; M rows of stride TRSV_TBP,
 // X rows of stride xs (16-byte aligned), out rows of stride os. All threads of the CTA call it.
-template <int KR, int TPR, bool SUB>
-__device__ __forceinline__ void tile_mul(const cpx<float> *M, int nrows, int kdim, const cpx<float> *X, int xs,
-                                         cpx<float> *out, int os)
+template <int KR, int TPR, bool SUB, typename R>
+__device__ __forceinline__ void tile_mul(const cpx<R> *M, int nrows, int kdim, const cpx<R> *X, int xs, cpx<R> *out,
+                                         int os)
 {
-    typedef cpx<float> C;
+    typedef cpx<R> C;
     const int r = threadIdx.x / TPR, h = threadIdx.x % TPR;
     C acc[KR];
 #pragma unroll
-    for (int c = 0; c < KR; ++c) acc[c] = mk<float>(0, 0);
+    for (int c = 0; c < KR; ++c) acc[c] = mk<R>(0, 0);
     if (r < nrows) {
         const C *row = M + (size_t)r * TRSV_TBP;
 #pragma unroll 2
         for (int k = h; k < kdim; k += TPR) {
             const C v = row[k];
-            const float4 *x = reinterpret_cast<const float4 *>(X + (size_t)k * xs);
+            if constexpr (sizeof(R) == 4) {                  // y as 16-byte pairs
+                const float4 *x = reinterpret_cast<const float4 *>(X + (size_t)k * xs);
 #pragma unroll
-            for (int c2 = 0; c2 < (KR + 1) / 2; ++c2) {
-                const float4 y = x[c2];
-                cfma<float>(acc[2 * c2], v, mk<float>(y.x, y.y));
-                if (2 * c2 + 1 < KR) cfma<float>(acc[2 * c2 + 1], v, mk<float>(y.z, y.w));
+                for (int c2 = 0; c2 < (KR + 1) / 2; ++c2) {
+                    const float4 y = x[c2];
+                    cfma<float>(acc[2 * c2], v, mk<float>(y.x, y.y));
+                    if (2 * c2 + 1 < KR) cfma<float>(acc[2 * c2 + 1], v, mk<float>(y.z, y.w));
+                }
+            } else {                                         // one 16-byte entry
+                const double2 *x = reinterpret_cast<const double2 *>(X + (size_t)k * xs);
+#pragma unroll
+                for (int c = 0; c < KR; ++c) {
+                    const double2 y = x[c];
+                    cfma<double>(acc[c], v, mk<double>(y.x, y.y));
+                }
             }
         }
     }
@@ -1442,27 +1456,28 @@ __device__ __forceinline__ void tile_mul(const cpx<float> *M, int nrows, int kdi
     }
 }
 
-template <int KR>
-__global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int vec16)
+template <typename R, int KR>
+__global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<R> a, int vec16)
 {
-    typedef cpx<float> C;
+    typedef cpx<R> C;
+    constexpr int RT = trsv_rt<R>();
     extern __shared__ __align__(16) unsigned char tq_raw[];
     const int G = gridDim.x, g = blockIdx.x, nb = a.nb, nrhs = a.nrhs, n = a.n;
     const int epoch = *(volatile const int *)a.epoch_ptr;
     const int per = (nb + G - 1) / G, bb0 = g * per, bb1 = min(nb, bb0 + per);
     const int R0 = bb0 * TB, R1 = min(n, bb1 * TB), nr = max(0, R1 - R0);
-    const int nw = per <= 2 ? per : 1;                                      // inverse buffers
-    C *tile = reinterpret_cast<C *>(tq_raw);                                // [2][TRSV_RT][TRSV_TBP]
-    C *Wt = tile + 2 * TRSV_RT * TRSV_TBP;                                  // [nw][TB][TRSV_TBP], transposed
+    const int nw = per <= trsv_nwmax<R>() ? per : 1;                        // inverse buffers
+    C *tile = reinterpret_cast<C *>(tq_raw);                                // [2][RT][TRSV_TBP]
+    C *Wt = tile + 2 * RT * TRSV_TBP;                                       // [nw][TB][TRSV_TBP], transposed
     C *Yb = Wt + (size_t)nw * TB * TRSV_TBP;                                // [TB][TRSV_YS]
     C *T = Yb + TB * TRSV_YS;                                               // [per * TB][TRSV_TS]
     __shared__ int ok;
     if (nr == 0) return;
     for (int e = threadIdx.x; e < nr * TRSV_TS; e += blockDim.x) {
         const int r = e / TRSV_TS, c = e % TRSV_TS;
-        T[e] = c < nrhs ? ldc<float>(a.Tin, (size_t)(R0 + r) * nrhs + c) : mk<float>(0, 0);
+        T[e] = c < nrhs ? ldc<R>(a.Tin, (size_t)(R0 + r) * nrhs + c) : mk<R>(0, 0);
     }
-    for (int e = threadIdx.x; e < TB * TRSV_YS; e += blockDim.x) Yb[e] = mk<float>(0, 0);
+    for (int e = threadIdx.x; e < TB * TRSV_YS; e += blockDim.x) Yb[e] = mk<R>(0, 0);
     if (threadIdx.x == 0) ok = 1;
     const C *Ac = reinterpret_cast<const C *>(a.A);
     auto blk = [&](int st) { return a.backward ? nb - 1 - st : st; };
@@ -1479,15 +1494,20 @@ __global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int ve
         int ra = 0, rb = 0;
         while (ls <= s_last) {
             rows_of(blk(ls), ra, rb);
-            const int nch = rb > ra ? (rb - ra + TRSV_RT - 1) / TRSV_RT : 0;
+            const int nch = rb > ra ? (rb - ra + RT - 1) / RT : 0;
             if (lc < nch) break;
             ++ls; lc = 0;
         }
         if (ls <= s_last) {
             const int b = blk(ls), b0 = b * TB, bs = min(TB, n - b0);
-            const int r0 = ra + lc * TRSV_RT, r1 = min(rb, r0 + TRSV_RT);
-            C *dst = tile + (size_t)(issued & 1) * TRSV_RT * TRSV_TBP;
-            if (vec16) {                                                    // a warp a row: lane q copies 16 bytes
+            const int r0 = ra + lc * RT, r1 = min(rb, r0 + RT);
+            C *dst = tile + (size_t)(issued & 1) * RT * TRSV_TBP;
+            if constexpr (sizeof(R) == 8) {                                 // 16 bytes a column: 64 threads a row
+                const int q = threadIdx.x & 63;
+                if (q < bs)
+                    for (int r = threadIdx.x >> 6; r < r1 - r0; r += TRSV_NT / 64)
+                        cp_async16(dst + (size_t)r * TRSV_TBP + q, Ac + (size_t)(r0 + r) * a.lda + b0 + q);
+            } else if (vec16) {                                             // a warp a row: lane q copies 16 bytes
                 const int q = threadIdx.x & 31;                             // (an odd last column alone, 8 bytes)
                 if (2 * q < bs)
                     for (int r = threadIdx.x >> 5; r < r1 - r0; r += TRSV_NT / 32) {
@@ -1508,16 +1528,28 @@ __global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int ve
     };
     // block b's inverse, transposed: Wt[rr][k] = W_b[k][rr] (W_b row-major TB x TB; 16-byte loads, one round trip)
     auto stage_w = [&](int b, C *dst) {
-        const float4 *W = reinterpret_cast<const float4 *>(
-            a.inv + 2 * ((size_t)b * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB)));
-        float4 v[TB * TB / 2 / TRSV_NT];
+        const R *Wr = a.inv + 2 * ((size_t)b * 2 * TB * TB + (a.backward ? 0 : (size_t)TB * TB));
+        if constexpr (sizeof(R) == 4) {
+            const float4 *W = reinterpret_cast<const float4 *>(Wr);
+            float4 v[TB * TB / 2 / TRSV_NT];
 #pragma unroll
-        for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) v[i] = __ldg(W + threadIdx.x + TRSV_NT * i);
+            for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) v[i] = __ldg(W + threadIdx.x + TRSV_NT * i);
 #pragma unroll
-        for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) {
-            const int e = 2 * (threadIdx.x + TRSV_NT * i), k = e / TB, rr = e % TB;   // (k, rr), (k, rr + 1)
-            dst[(size_t)rr * TRSV_TBP + k] = mk<float>(v[i].x, v[i].y);
-            dst[(size_t)(rr + 1) * TRSV_TBP + k] = mk<float>(v[i].z, v[i].w);
+            for (int i = 0; i < TB * TB / 2 / TRSV_NT; ++i) {
+                const int e = 2 * (threadIdx.x + TRSV_NT * i), k = e / TB, rr = e % TB;   // (k, rr), (k, rr + 1)
+                dst[(size_t)rr * TRSV_TBP + k] = mk<float>(v[i].x, v[i].y);
+                dst[(size_t)(rr + 1) * TRSV_TBP + k] = mk<float>(v[i].z, v[i].w);
+            }
+        } else {
+            const double2 *W = reinterpret_cast<const double2 *>(Wr);
+            double2 v[TB * TB / TRSV_NT];
+#pragma unroll
+            for (int i = 0; i < TB * TB / TRSV_NT; ++i) v[i] = __ldg(W + threadIdx.x + TRSV_NT * i);
+#pragma unroll
+            for (int i = 0; i < TB * TB / TRSV_NT; ++i) {
+                const int e = threadIdx.x + TRSV_NT * i, k = e / TB, rr = e % TB;
+                dst[(size_t)rr * TRSV_TBP + k] = mk<double>(v[i].x, v[i].y);
+            }
         }
     };
     auto wbuf = [&](int b) { return Wt + (size_t)(nw == 1 ? 0 : b - bb0) * TB * TRSV_TBP; };
@@ -1541,17 +1573,18 @@ __global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int ve
             __syncthreads();
             if (!ok) { cp_async_wait0(); return; }
             {                                                               // another CTA's values: past L1,
-                const float *p = a.Xout + 2 * (size_t)b0 * nrhs;            // all loads before the stores
-                float2 v[TB * 16 / TRSV_NT];
+                typedef typename vec2_of<R>::type V2;                       // all loads before the stores
+                const V2 *p = reinterpret_cast<const V2 *>(a.Xout) + (size_t)b0 * nrhs;
+                V2 v[TB * 16 / TRSV_NT];
 #pragma unroll
                 for (int i = 0; i < TB * 16 / TRSV_NT; ++i) {
                     const int e = threadIdx.x + TRSV_NT * i;
-                    v[i] = e < bs * nrhs ? __ldcg(reinterpret_cast<const float2 *>(p) + e) : make_float2(0.f, 0.f);
+                    if (e < bs * nrhs) v[i] = __ldcg(p + e);
                 }
 #pragma unroll
                 for (int i = 0; i < TB * 16 / TRSV_NT; ++i) {
                     const int e = threadIdx.x + TRSV_NT * i;
-                    if (e < bs * nrhs) Yb[(e / nrhs) * TRSV_YS + e % nrhs] = mk<float>(v[i].x, v[i].y);
+                    if (e < bs * nrhs) Yb[(e / nrhs) * TRSV_YS + e % nrhs] = mk<R>(v[i].x, v[i].y);
                 }
             }
         } else {
@@ -1560,7 +1593,7 @@ __global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int ve
                                               TRSV_YS);
             __syncthreads();
             for (int e = threadIdx.x; e < bs * nrhs; e += blockDim.x)
-                stc<float>(a.Xout, (size_t)b0 * nrhs + e, Yb[(e / nrhs) * TRSV_YS + e % nrhs]);
+                stc<R>(a.Xout, (size_t)b0 * nrhs + e, Yb[(e / nrhs) * TRSV_YS + e % nrhs]);
             __syncthreads();
             if (threadIdx.x == 0) {                                         // the CTA's stores, then the flag
                 __threadfence();
@@ -1571,13 +1604,12 @@ __global__ void __launch_bounds__(TRSV_NT) k_trsv_pipe(TrsvArgs<float> a, int ve
         }
         int ra, rb;
         rows_of(b, ra, rb);
-        for (int r0 = ra; r0 < rb; r0 += TRSV_RT) {
+        for (int r0 = ra; r0 < rb; r0 += RT) {
             issue_next();                                                   // the next task's tile, other buffer
             cp_async_wait1();                                               // this task's tile has landed
             __syncthreads();
-            tile_mul<KR, TRSV_NT / TRSV_RT, true>(tile + (size_t)(used & 1) * TRSV_RT * TRSV_TBP,
-                                                  min(rb, r0 + TRSV_RT) - r0, bs, Yb, TRSV_YS,
-                                                  T + (size_t)(r0 - R0) * TRSV_TS, TRSV_TS);
+            tile_mul<KR, TRSV_NT / RT, true>(tile + (size_t)(used & 1) * RT * TRSV_TBP, min(rb, r0 + RT) - r0, bs,
+                                             Yb, TRSV_YS, T + (size_t)(r0 - R0) * TRSV_TS, TRSV_TS);
             ++used;
             __syncthreads();                                                // the buffer is the next copy's
         }
@@ -2031,14 +2063,17 @@ static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B,
     TrsvArgs<R> fa{A, lda, n, nb, inv, B, W1, nrhs, 0, flags, epoch, err};          // U^T y = b: B -> W1
     TrsvArgs<R> ba{A, lda, n, nb, inv, W1, W2, nrhs, 1, flags + nb, epoch, err};    // L^T z = y: W1 -> W2
     const int per = (nb + G - 1) / G;
-    if (std::is_same<R, float>::value && per <= TRSV_MAXPER) {
-        // complex64: the factor tiles through shared memory (cp.async, 16-byte pieces where rows allow); the
-        // kernel for the smallest compile-time column count >= nrhs
-        const size_t psm = trsv_pipe_smem(per);
+    int smem_optin = 0, dev = 0;
+    M25_CHECK(cudaGetDevice(&dev));
+    M25_CHECK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (per <= TRSV_MAXPER && trsv_pipe_smem<R>(per) + 256 <= (size_t)smem_optin) {
+        // the factor tiles through shared memory (cp.async, 16-byte pieces where rows allow); the kernel for the
+        // smallest compile-time column count >= nrhs
+        const size_t psm = trsv_pipe_smem<R>(per);
         int vec16 = (lda % 2 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0);
-        const void *kf = nrhs <= 1 ? (const void *)k_trsv_pipe<1> : nrhs <= 2 ? (const void *)k_trsv_pipe<2> :
-                         nrhs <= 4 ? (const void *)k_trsv_pipe<4> : nrhs <= 8 ? (const void *)k_trsv_pipe<8> :
-                         (const void *)k_trsv_pipe<16>;
+        const void *kf = nrhs <= 1 ? (const void *)k_trsv_pipe<R, 1> : nrhs <= 2 ? (const void *)k_trsv_pipe<R, 2> :
+                         nrhs <= 4 ? (const void *)k_trsv_pipe<R, 4> : nrhs <= 8 ? (const void *)k_trsv_pipe<R, 8> :
+                         (const void *)k_trsv_pipe<R, 16>;
         M25_CHECK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
         void *fargs[] = {&fa, &vec16};
         M25_CHECK(cudaLaunchCooperativeKernel(kf, dim3(G), dim3(TRSV_NT), fargs, psm, s));

@@ -345,6 +345,35 @@ def test_complex64_solves_over_several_blocks_a_cta(n, nrhs):
         assert err < 1e-4, err
 
 
+@pytest.mark.parametrize('n,nrhs', [(9509, 1), (18788, 8), (19000, 16)])
+def test_complex128_solves_over_several_blocks_a_cta(n, nrhs):
+    """The complex128 solves through the same pipelined kernel (32-row factor tiles, one inverse buffer) where the
+    CTAs own one and two 64-row blocks, 1 to 16 right-hand sides: against cuSOLVER's solve of the same Z, at double
+    precision's bar."""
+    from mom25d_b200 import _lib
+    g = torch.Generator(device='cuda').manual_seed(n)
+    Z = torch.complex(torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64),
+                      torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64))
+    Z.diagonal().add_(4 * n ** 0.5)
+    R = torch.complex(torch.randn(n, nrhs, generator=g, device='cuda', dtype=torch.float64),
+                      torch.randn(n, nrhs, generator=g, device='cuda', dtype=torch.float64))
+    x = torch.linalg.solve(Z, R)
+    F = Z.clone()
+    ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
+    nb = int(_lib.lib().m25_getrf_workspace(n, 0))
+    work = torch.empty(nb, dtype=torch.uint8, device='cuda')
+    _lib.check(_lib.lib().m25_getrf(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 0, 0, _lib.P(work),
+                                    ctypes.c_size_t(nb), _lib.stream_ptr()))
+    del work
+    for _ in range(2):                                               # twice: the flags' epochs
+        X = R.clone()
+        _lib.check(_lib.lib().m25_getrs(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 0, _lib.P(X), nrhs,
+                                        _lib.stream_ptr()))
+        _lib.sync_check()
+        err = (X - x).abs().max().item() / x.abs().max().item()
+        assert err < 1e-11, err
+
+
 @pytest.mark.parametrize('k', [1, 3, 8])
 def test_gmres_batched_matches_a_direct_solve(small, k):
     """The refinement's GMRES (device Arnoldi steps, host least squares) on a dense system with a nearby
