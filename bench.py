@@ -236,6 +236,7 @@ def run_gpu(args, rank, world):
     ds.timings, ds.attempts = {}, []
     ev0.record(stream)
     for i in range(args.steps):
+        ph0 = dict(ds.timings) if args.verbose else None
         ms, lms, X = step_device(mine[i % len(mine)], 'mixed')
         lat.append(ms); iters.append(max(ds.iters) if ds.iters else 0)
         if lms is not None:
@@ -245,8 +246,10 @@ def run_gpu(args, rank, world):
         kept_X.append(X)                    # compared with the FP64 solve of the same frequency below
         if args.verbose:
             rh = getattr(ds, 'res_hist', [])
+            ph = {k: 1000 * (v - ph0.get(k, 0.0)) for k, v in ds.timings.items() if v - ph0.get(k, 0.0) > 5e-4}
             print(f"step {i}: {mine[i % len(mine)] / 1e9:.4g} GHz {ds.last_path:22s} {iters[-1]:3d} iterations "
-                  f"{ms:8.1f} ms  residual by step: " + ' '.join(f"{x:.0e}" for x in rh[1::3]), file=sys.stderr)
+                  f"{ms:8.1f} ms  phases " + ' '.join(f"{k} {v:.0f}" for k, v in ph.items()) +
+                  "  residual by step: " + ' '.join(f"{x:.0e}" for x in rh[1::3]), file=sys.stderr)
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = clk.stop()

@@ -49,6 +49,8 @@ REUSE_GIVE_UP = (10, 0.05)   # a reused factor's GMRES ends from step 10 where a
 FRESH_STAGNATION = (10, 0.5)  # a fresh factor's GMRES ends at step 10 where a residual has not halved since step 1
                              # (measured on the routed board: at 0.5 GHz it stays at 2e-3 for all 30 steps; at 0.67 GHz
                              # it is 5x lower by step 10 and converges at 27)
+REACH_WINDOW = float(0.5 * np.log(2.0))  # _reach_at: the attempts within half an octave of f set its reach (an
+                             # octave let the 4.07 GHz failure of the routed board stop the reuses at 2.24 GHz)
 DOUBLE_REACH = float(np.log(1.6))  # |ln f / f0| within which the kept double factor preconditions a double solve
 DOUBLE_UP = 1.6              # after a complex64 failure at f0, the frequencies up to this x f0 with the kept double factor
                              # within reach go to it directly, past the reference's MIXED_RETRY: a complex64 factor is
@@ -380,13 +382,14 @@ class DirectSolver:
 
     def _reach_at(self, f):
         """The reach at f: the reference's rule (fast.py:989-994: a quick success widens it to 1.25 d, a failure
-        narrows it to 0.8 d) replayed over the attempts within an octave of f, in the order they were made. The
+        narrows it to 0.8 d) replayed over the attempts within half an octave of f (REACH_WINDOW), in the order
+        they were made. The
         reference learns one reach for the whole band; how fast Z moves with f depends on where in the band f is
         (measured on the routed board: reuses converge at 1.57x the kept frequency around 1-3 GHz and fail at
         1.16x above 5 GHz), so a failure at 6 GHz no longer stops the reuses at 2 GHz."""
         r = self.reach
         for fa, d, ok, iters, cap in self.reach_log:
-            if abs(np.log(f / fa)) > np.log(2.0):
+            if abs(np.log(f / fa)) > REACH_WINDOW:
                 continue
             if ok and iters <= cap // 2:
                 r = max(r, 1.25 * d)
