@@ -182,8 +182,10 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, b
 template <int KMAX>
 constexpr int zgemm_jc() { return KMAX >= 16 ? 128 : 256; }
 
+// 8 and 16 columns: RW rows a warp in the registers of one CTA an SM (4 and 2 rows: 1.79 and 4.14 ms at N = 18,788
+// against 1.82 and 5.32 for 2 and 1 rows at two CTAs an SM, which spilled); 2 and 4 columns: two CTAs an SM
 template <int KMAX, int RW>
-__global__ void __launch_bounds__(256, 2) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
+__global__ void __launch_bounds__(256, KMAX >= 8 ? 1 : 2) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
                                                          const double *__restrict__ X, int k, double *__restrict__ Y)
 {
     constexpr int JC = zgemm_jc<KMAX>();
@@ -416,8 +418,8 @@ extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double 
     // fewer rows a warp as the columns grow (registers: two CTAs an SM keep enough loads of Z in flight)
     if (k <= 2) return zgemm_launch<2, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     if (k <= 4) return zgemm_launch<4, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
-    if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
-    return zgemm_launch<16, 1>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    if (k <= 8) return zgemm_launch<8, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    return zgemm_launch<16, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
 }
 
 extern "C" int m25_dotc_multi(const double *d_V, int nv, long N, int k, const double *d_W, double *d_out, void *stream)
