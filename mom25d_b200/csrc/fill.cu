@@ -160,8 +160,10 @@ __device__ __forceinline__ void fill_far_tile(R *Z, long ld, const m25_mesh &g, 
     }
 }
 
+// four CTAs an SM (64 registers; 88 let two): the tile's phases end in barriers, and the other CTAs' warps fill
+// those stalls (routed board, N = 18,788: the FP64 fill phase 15.5 -> 12.3 ms; three CTAs 12.6)
 template <typename R, typename TB>
-__global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB tb, double w)
+__global__ void __launch_bounds__(256, 4) k_fill_far(R *Z, long ld, m25_mesh g, TB tb, double w)
 {
     fill_far_tile<R, TB>(Z, ld, g, tb, w);
 }
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(256) k_fill_far(R *Z, long ld, m25_mesh g, TB 
 // Several frequencies of one board in one launch: grid z is the frequency, each with its own Z, tables and w (the
 // batched sweep: the far part of every frequency's Z, the tables of all of them resident).
 template <typename R, typename TB>
-__global__ void __launch_bounds__(256) k_fill_far_multi(R *const *Zs, long ld, m25_mesh g, const TB *tbs,
+__global__ void __launch_bounds__(256, 4) k_fill_far_multi(R *const *Zs, long ld, m25_mesh g, const TB *tbs,
                                                         const double *ws)
 {
     const int f = blockIdx.z;
