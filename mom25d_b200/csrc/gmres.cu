@@ -182,10 +182,11 @@ __device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, b
 template <int KMAX>
 constexpr int zgemm_jc() { return KMAX >= 16 ? 128 : 256; }
 
-// 8 and 16 columns: RW rows a warp in the registers of one CTA an SM (4 and 2 rows: 1.79 and 4.14 ms at N = 18,788
-// against 1.82 and 5.32 for 2 and 1 rows at two CTAs an SM, which spilled); 2 and 4 columns: two CTAs an SM
+// 16 columns: two rows a warp in the registers of one CTA an SM (4.14 ms at N = 18,788 against 5.32 for one row at
+// two CTAs an SM, which spilled); up to 8 columns two CTAs an SM (8 columns with four rows at one CTA: 674 against
+// 619 us at N = 9,600)
 template <int KMAX, int RW>
-__global__ void __launch_bounds__(256, KMAX >= 8 ? 1 : 2) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
+__global__ void __launch_bounds__(256, RW * KMAX >= 32 ? 1 : 2) k_zgemm_skinny(const double *__restrict__ Z, long ld, int n,
                                                          const double *__restrict__ X, int k, double *__restrict__ Y)
 {
     constexpr int JC = zgemm_jc<KMAX>();
@@ -418,7 +419,7 @@ extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double 
     // fewer rows a warp as the columns grow (registers: two CTAs an SM keep enough loads of Z in flight)
     if (k <= 2) return zgemm_launch<2, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     if (k <= 4) return zgemm_launch<4, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
-    if (k <= 8) return zgemm_launch<8, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     return zgemm_launch<16, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
 }
 
