@@ -313,9 +313,7 @@ class DirectSolver:
         E = E.reshape(N, -1).contiguous()
         self.iters = []
         self.last_lu_ms = self.last_lu_c64_ms = None
-        near_double = (self.kept64 is not None and f <= DOUBLE_UP * self.mixed_failed and
-                       abs(np.log(f / self.kept64[0])) <= DOUBLE_REACH)
-        if precision == 'mixed' and (f <= MIXED_RETRY * self.mixed_failed or near_double):
+        if precision == 'mixed' and self._double_band(f):
             precision = 'double'                          # fast.py:740: near a failure, double
             if self._hybrid_fits():
                 return self._solve_double_near(f, E)
@@ -366,6 +364,15 @@ class DirectSolver:
         kept = sum(k[1]['bytes'] for k in self.kept)
         cap = self.keep if self.keep is not None else min(KEEP_HBM[0], int(KEEP_HBM[1] * total // (8.0 * N * N)))
         return int(min(cap, (0.9 * (free + kept) - 0.4e9) // (8.0 * N * N)))
+
+    def _double_band(self, f):
+        """Whether a mixed request at f is solved in double: up to MIXED_RETRY x the highest complex64 failure (the
+        reference's rule, fast.py:740), and up to DOUBLE_UP x it where the kept double factor is within
+        DOUBLE_REACH of f."""
+        if f <= MIXED_RETRY * self.mixed_failed:
+            return True
+        return (self.kept64 is not None and f <= DOUBLE_UP * self.mixed_failed and
+                abs(np.log(f / self.kept64[0])) <= DOUBLE_REACH)
 
     def forget(self):
         """A new sweep: no kept factors, nothing learnt."""
