@@ -63,6 +63,17 @@ template <typename R> __device__ __forceinline__ void stc(R *p, size_t i, cpx<R>
     reinterpret_cast<V *>(p)[i] = v;
 }
 
+// ---- FP64 tensor-core product (mma.sync; tcgen05 has no FP64 kind) ------------------------------------------------
+// D (16 x 8) += A (16 x 8, row) B (8 x 8, col), FP64. Lane l = 4 g + t holds A[g][t], A[g + 8][t], A[g][t + 4],
+// A[g + 8][t + 4]; B[t][g], B[t + 4][g]; D[g][2 t], D[g][2 t + 1], D[g + 8][2 t], D[g + 8][2 t + 1].
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2])
+{
+    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
 // ---- error plumbing ---------------------------------------------------------------------------------------------------
 void m25_set_error(const std::string &msg);
 int m25_cuda_status(cudaError_t e, const char *where);

@@ -260,6 +260,94 @@ static int zgemm_launch(const double *d_Z, long ld, int n, const double *d_X, in
     return M25_OK;
 }
 
+// The same product for up to 8 columns on the FP64 tensor cores (above 4 columns the CUDA-core kernel is bound by
+// its four FP64 FMAs a complex term, not by HBM): a warp takes 16 rows of Z and walks its share of the row in steps
+// of 8 columns, one m16n8k8 f64 MMA per real part (Yr += Zr Xr - Zi Xi, Yi += Zr Xi + Zi Xr). The MMA's K slots are
+// matched to the columns as slot t <-> column 2 t, slot t + 4 <-> column 2 t + 1 (the same in A and in B), so that
+// each lane reads two adjacent complex entries (32 bytes) of its two rows and the four lanes of a row 128 contiguous
+// bytes; UNR steps of loads are issued before their MMAs. X (read by every warp) comes through the read-only cache.
+// ks warps (1, 2 or 4) share a group of 16 rows, each a contiguous share of the columns, their partial sums added
+// through shared memory, so that small n still fills the SMs. kk <= 8 columns of X and Y, row strides ldx and ldy
+// (a 16-column product is two such passes).
+template <int UNR>
+__global__ void __launch_bounds__(256, 1) k_zgemm_dmma8(const double *__restrict__ Z, long ld, int n,
+                                                        const double *__restrict__ X, int kk, int ldx,
+                                                        double *__restrict__ Y, int ldy, int ks)
+{
+    __shared__ double red[8][32][8];                                  // [warp][lane][dr 0..3, di 0..3]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int rg = warp / ks, part = warp % ks;
+    const long row0 = ((long)blockIdx.x * (8 / ks) + rg) * 16;
+    const double2 *Z2 = reinterpret_cast<const double2 *>(Z);
+    const double2 *X2 = reinterpret_cast<const double2 *>(X);
+    const long ra = row0 + g, rb = row0 + g + 8;
+    const bool va = ra < n, vb = rb < n, colok = g < kk;
+    const double2 *za = Z2 + (size_t)(va ? ra : 0) * ld, *zb = Z2 + (size_t)(vb ? rb : 0) * ld;
+    const double2 zero = make_double2(0.0, 0.0);
+    double dr[4] = {0, 0, 0, 0}, di[4] = {0, 0, 0, 0};
+    const long step = 8L * UNR, share = ((n + step - 1) / step + ks - 1) / ks * step;
+    const long jbeg = part * share, jend = min((long)n, jbeg + share);
+    for (long j0 = row0 < n ? jbeg : jend; j0 < jend; j0 += step) {
+        double2 a[UNR][4], b[UNR][2];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const long j = j0 + 8 * u + 2 * t;
+            const bool j0ok = j < jend, j1ok = j + 1 < jend;
+            a[u][0] = va && j0ok ? __ldcs(za + j) : zero;                 // A[g][t]
+            a[u][1] = vb && j0ok ? __ldcs(zb + j) : zero;                 // A[g + 8][t]
+            a[u][2] = va && j1ok ? __ldcs(za + j + 1) : zero;             // A[g][t + 4]
+            a[u][3] = vb && j1ok ? __ldcs(zb + j + 1) : zero;             // A[g + 8][t + 4]
+            b[u][0] = colok && j0ok ? __ldg(X2 + (size_t)j * ldx + g) : zero;        // B[t][g]
+            b[u][1] = colok && j1ok ? __ldg(X2 + (size_t)(j + 1) * ldx + g) : zero;  // B[t + 4][g]
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const double ar[4] = {a[u][0].x, a[u][1].x, a[u][2].x, a[u][3].x};
+            const double ai[4] = {a[u][0].y, a[u][1].y, a[u][2].y, a[u][3].y};
+            const double br[2] = {b[u][0].x, b[u][1].x}, bi[2] = {b[u][0].y, b[u][1].y};
+            const double nbi[2] = {-b[u][0].y, -b[u][1].y};
+            dmma_16x8x8(dr, ar, br);
+            dmma_16x8x8(dr, ai, nbi);
+            dmma_16x8x8(di, ar, bi);
+            dmma_16x8x8(di, ai, br);
+        }
+    }
+    if (ks > 1) {                                                     // the row group's shares added by its first warp
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { red[warp][lane][q] = dr[q]; red[warp][lane][4 + q] = di[q]; }
+        __syncthreads();
+        if (part != 0) return;
+        for (int p = 1; p < ks; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { dr[q] += red[warp + p][lane][q]; di[q] += red[warp + p][lane][4 + q]; }
+    }
+    double2 *Y2 = reinterpret_cast<double2 *>(Y);                    // D[g][2t], D[g][2t + 1], D[g + 8][2t], ...
+    const int c0 = 2 * t, c1 = 2 * t + 1;
+    if (va && c0 < kk) Y2[(size_t)ra * ldy + c0] = make_double2(dr[0], di[0]);
+    if (va && c1 < kk) Y2[(size_t)ra * ldy + c1] = make_double2(dr[1], di[1]);
+    if (vb && c0 < kk) Y2[(size_t)rb * ldy + c0] = make_double2(dr[2], di[2]);
+    if (vb && c1 < kk) Y2[(size_t)rb * ldy + c1] = make_double2(dr[3], di[3]);
+}
+
+// ks: the fewest warps a row group that give three quarters of the SMs or more a CTA (8 warps an SM)
+static int zdmma8_launch(const double *d_Z, long ld, int n, const double *d_X, int kk, int ldx, double *d_Y, int ldy,
+                         cudaStream_t s)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        M25_CHECK(cudaGetDevice(&dev));
+        M25_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const long groups = (n + 15) / 16;
+    int ks = 1;
+    while (ks < 4 && 4 * ((groups * ks + 7) / 8) < 3 * (long)sms) ks *= 2;
+    const long ctas = (groups * ks + 7) / 8;
+    k_zgemm_dmma8<4><<<(unsigned)ctas, 256, 0, s>>>(d_Z, ld, n, d_X, kk, ldx, d_Y, ldy, ks);
+    M25_LAUNCH_CHECK("k_zgemm_dmma8");
+    return M25_OK;
+}
+
 // The Gram-Schmidt step of the batched GMRES against all basis vectors at once (classical Gram-Schmidt, applied
 // twice by the caller): out[i, c] = sum_n conj(V_i[n, c]) W[n, c] for i < nv (V: nv consecutive N x k blocks), one
 // grid row of blocks per vector; W -= sum_i V_i h[i] (h: nv x k complex, per column).
@@ -419,8 +507,15 @@ extern "C" int m25_zgemm_skinny(const double *d_Z, long ld, int n, const double 
     // fewer rows a warp as the columns grow (registers: two CTAs an SM keep enough loads of Z in flight)
     if (k <= 2) return zgemm_launch<2, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
     if (k <= 4) return zgemm_launch<4, 4>(d_Z, ld, n, d_X, k, d_Y, S(stream));
-    if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
-    return zgemm_launch<16, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+    if (const char *e = getenv("M25_ZGEMM_DMMA")) {
+        if (atoi(e) == 0) {                                  // (the CUDA-core kernel: comparisons)
+            if (k <= 8) return zgemm_launch<8, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+            return zgemm_launch<16, 2>(d_Z, ld, n, d_X, k, d_Y, S(stream));
+        }
+    }
+    int rc = zdmma8_launch(d_Z, ld, n, d_X, std::min(k, 8), k, d_Y, k, S(stream));   // columns 0 .. 8
+    if (rc || k <= 8) return rc;
+    return zdmma8_launch(d_Z, ld, n, d_X + 16, k - 8, k, d_Y + 16, k, S(stream));   // columns 8 .. k
 }
 
 extern "C" int m25_dotc_multi(const double *d_V, int nv, long N, int k, const double *d_W, double *d_out, void *stream)

@@ -999,15 +999,6 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
 #define ZD_SA (ZD_BM + 2)          // A slice [k][m], complex: a row stride = 2 mod 8 keeps the 16-byte reads conflict-free
 #define ZD_SB (ZD_BK + 4)          // B slice [n][k], complex: 4 mod 8
 
-// D (16 x 8) += A (16 x 8, row) B (8 x 8, col), FP64. Lane l = 4 g + t holds A[g][t], A[g + 8][t], A[g][t + 4],
-// A[g + 8][t + 4]; B[t][g], B[t + 4][g]; D[g][2 t], D[g][2 t + 1], D[g + 8][2 t], D[g + 8][2 t + 1].
-__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2])
-{
-    asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};"
-        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
-}
 
 __device__ __forceinline__ void cp_async16_zfill_lu(void *smem, const void *gmem, bool valid)
 {
