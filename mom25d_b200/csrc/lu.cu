@@ -974,17 +974,25 @@ __global__ void __launch_bounds__(256) k_gemm_update(R *Cm, const R *Am, const R
         __syncthreads();
         buf ^= 1;
     }
+    // C -= the product, four rows of outputs at a time: their 16 values of C read before any is written (a load ->
+    // store chain a value serialised the memory latency 32 times a thread)
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        int m = m0 + ty + 16 * i;
-        if (m >= M) continue;
+    for (int i0 = 0; i0 < 8; i0 += 4) {
+        C cv[4][4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int nn = n0 + tx + 16 * j;
-            if (nn >= N) continue;
-            size_t o = (size_t)nn * lda + m;
-            stc<R>(Cm, o, ldc<R>(Cm, o) - acc[i][j]);
-        }
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int m = m0 + ty + 16 * (i0 + i), nn = n0 + tx + 16 * j;
+                cv[i][j] = (m < M && nn < N) ? ldc<R>(Cm, (size_t)nn * lda + m) : mk<R>(0, 0);
+            }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int m = m0 + ty + 16 * (i0 + i), nn = n0 + tx + 16 * j;
+                if (m < M && nn < N) stc<R>(Cm, (size_t)nn * lda + m, cv[i][j] - acc[i0 + i][j]);
+            }
     }
 }
 
@@ -1091,24 +1099,29 @@ __global__ void __launch_bounds__(128, 2) k_zgemm_dmma(double *Cm, const double 
         buf ^= 1;
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // C -= the product: fragment q of tile (i, j) is row g (+ 8 for q >= 2), column 2 t + (q & 1)
+    // C -= the product: fragment q of tile (i, j) is row g (+ 8 for q >= 2), column 2 t + (q & 1). By 16-row tile,
+    // its 16 values of C read before any is written (a load -> store chain a value serialised the memory latency
+    // 32 times a thread; the complex128 LU at N = 18,788 took 705 ms with it, 626 ms without)
+    double2 *C2 = reinterpret_cast<double2 *>(Cm);
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 2; ++i) {
+        double2 cv[4][4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int m = m0 + wm + 16 * i + fg + (q >= 2 ? 8 : 0);
-            if (m >= M) continue;
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const int nn = n0 + wn + 8 * j + 2 * ft + (q & 1);
-                if (nn >= N) continue;
-                double2 *p = reinterpret_cast<double2 *>(Cm) + (size_t)nn * lda + m;
-                double2 c = *p;
-                c.x -= cr[i][j][q];
-                c.y -= ci[i][j][q];
-                *p = c;
+                const int m = m0 + wm + 16 * i + fg + (q >= 2 ? 8 : 0), nn = n0 + wn + 8 * j + 2 * ft + (q & 1);
+                cv[q][j] = (m < M && nn < N) ? C2[(size_t)nn * lda + m] : make_double2(0.0, 0.0);
             }
-        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int m = m0 + wm + 16 * i + fg + (q >= 2 ? 8 : 0), nn = n0 + wn + 8 * j + 2 * ft + (q & 1);
+                if (m < M && nn < N) C2[(size_t)nn * lda + m] = make_double2(cv[q][j].x - cr[i][j][q],
+                                                                             cv[q][j].y - ci[i][j][q]);
+            }
+    }
 }
 
 template <typename R>
