@@ -261,7 +261,10 @@ int m25_get_lu_tuning(int n, int single, int *nb2, int *blocks);
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);
 /* The solves split for a factor that is solved with many times (the refinement's preconditioner, the backend's
  * solve(R)): m25_getrs_prepare inverts the factor's diagonal blocks once into d_aux (m25_getrs_aux_bytes) and
- * keeps the pivots there; m25_getrs_aux then solves like m25_getrs from d_aux. d_aux belongs to one factor. */
+ * keeps the pivots there; m25_getrs_aux then solves like m25_getrs from d_aux. d_aux belongs to one factor. For a
+ * complex64 factor of n >= 2048, d_aux also holds the inverses of its 256-row diagonal blocks and their couplings
+ * with the two blocks before them (six 256 x 256 matrices a block, 3 n 256 complex entries a triangle), with
+ * which solves of up to 8 right-hand sides take one product a block along their chain (M25_TRSV=pipe: not). */
 size_t m25_getrs_aux_bytes(int n, int single);
 int m25_getrs_prepare(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
                       size_t aux_bytes, void *stream);
@@ -270,8 +273,10 @@ int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void *d_aux, vo
  * stream-ordered allocator at every call; this variant uses a fixed file-scope device array of
  * M25_GETRS_NOALLOC_MAX_BYTES instead, for callers that must not have the library take device memory during a
  * call: a serving loop that admits requests by a fixed HBM budget, or a process whose memory is all reserved up
- * front. Same arguments and results as m25_getrs. Limit: n with m25_getrs_aux_bytes(n, single) above
- * M25_GETRS_NOALLOC_MAX_BYTES (about n = 26,000 complex64, 13,000 complex128) is rejected with M25_EINVAL and a
+ * front. Same arguments as m25_getrs and its results to rounding (it always solves by 64-row diagonal blocks).
+ * Limit: n whose data for those solves
+ * (inverses, permutation, work vectors, flags) is above M25_GETRS_NOALLOC_MAX_BYTES (about n = 26,000 complex64,
+ * 13,000 complex128) is rejected with M25_EINVAL and a
  * message. The first call on a device does the setup (it looks up the array's device address); make it before
  * any stream capture. The array is one per device and process: calls that overlap (other streams, other host
  * threads on the same device) race on it and must be serialised by the caller. A bounded wait that gave up is

@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, 'csrc')
 LIB = os.path.join(HERE, 'libmom25d_b200.so')
-SOURCES = ['capi.cu', 'green.cu', 'fill.cu', 'vias.cu', 'gmres.cu', 'lu.cu', 'umma.cu', 'noalloc.cu']
+SOURCES = ['capi.cu', 'green.cu', 'fill.cu', 'vias.cu', 'gmres.cu', 'lu.cu', 'umma.cu', 'noalloc.cu', 'trsv_sb.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-O3', '-std=c++17',
          '-Xcompiler', '-fPIC', '-shared', '-Xptxas', '-O3', '--expt-relaxed-constexpr']

@@ -2048,10 +2048,26 @@ static size_t aux_layout(int n, size_t *off_inv, size_t *off_perm, size_t *off_w
     return o;
 }
 
-extern "C" size_t m25_getrs_aux_bytes(int n, int single)
+// The 256-row-block solves (trsv_sb.cu): their data after the 64-row-block solves' in the same aux buffer
+bool m25_sb_enabled(int n, int single);
+size_t m25_sb_bytes(int n, int single);
+int m25_sb_prepare(const void *A, long lda, int n, int single, const void *inv64, void *sb, cudaStream_t s);
+int m25_sb_solve(const void *A, long lda, int n, int single, void *sb, const void *Tin, void *Xout, int nrhs,
+                 int backward, const int *epoch, int *err, cudaStream_t s);
+
+// the 64-row-block solves' data alone (the layout of m25_getrs_noalloc's fixed scratch)
+size_t m25_getrs_aux_bytes_basic(int n, int single)
 {
     size_t a, b, c;
     return single ? aux_layout<float>(n, &a, &b, &c) : aux_layout<double>(n, &a, &b, &c);
+}
+// where the 256-row-block solves' data starts in an aux buffer
+static size_t sb_offset(int n, int single) { return (m25_getrs_aux_bytes_basic(n, single) + 255) / 256 * 256; }
+
+extern "C" size_t m25_getrs_aux_bytes(int n, int single)
+{
+    const size_t sb = m25_sb_bytes(n, single);
+    return sb ? sb_offset(n, single) + sb : m25_getrs_aux_bytes_basic(n, single);
 }
 
 template <typename R>
@@ -2061,12 +2077,18 @@ static size_t trsv_smem(int n, int G)
     return sizeof(cpx<R>) * (TB * (TB + 1) + TB * 16 + (size_t)per * TB * 16);
 }
 
+// sb: the 256-row-block solves where m25_sb_enabled (their data after the basic layout); false keeps the basic
+// layout alone (m25_getrs_noalloc's fixed scratch)
 template <typename R>
 static int getrs_prepare_impl(const R *A, long lda, int n, const int *ipiv, unsigned char *aux, size_t aux_bytes,
-                              cudaStream_t s)
+                              cudaStream_t s, bool sb)
 {
     size_t oi, op, ow, of;
     M25_REQUIRE(aux_bytes >= aux_layout<R>(n, &oi, &op, &ow, &of), "m25_getrs_prepare: aux buffer too small");
+    const int single = sizeof(R) == 4;
+    const bool use_sb = sb && m25_sb_enabled(n, single);
+    const size_t basic = sb_offset(n, single);
+    if (use_sb) M25_REQUIRE(aux_bytes >= basic + m25_sb_bytes(n, single), "m25_getrs_prepare: aux buffer too small");
     const int nb = (n + TB - 1) / TB;
     const size_t ismem = 2 * sizeof(cpx<R>) * TB * (TB + 1);
     M25_CHECK(cudaFuncSetAttribute(k_block_inverses<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ismem));
@@ -2077,11 +2099,13 @@ static int getrs_prepare_impl(const R *A, long lda, int n, const int *ipiv, unsi
     k_perm_from_ipiv<<<1, 1024, sizeof(int) * n, s>>>(ipiv, n, (int *)(aux + op));
     M25_LAUNCH_CHECK("k_perm_from_ipiv");
     M25_CHECK(cudaMemsetAsync(aux + of, 0, sizeof(int) * (2 * nb + 32), s));
+    if (use_sb) return m25_sb_prepare(A, lda, n, single, aux + oi, aux + basic, s);
     return M25_OK;
 }
 
 template <typename R>
-static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B, int nrhs, cudaStream_t s, int *err)
+static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B, int nrhs, cudaStream_t s, int *err,
+                          bool sb)
 {
     size_t oi, op, ow, of;
     aux_layout<R>(n, &oi, &op, &ow, &of);
@@ -2090,6 +2114,20 @@ static int getrs_aux_impl(const R *A, long lda, int n, unsigned char *aux, R *B,
     R *W1 = (R *)(aux + ow), *W2 = W1 + 2 * (size_t)n * 16;
     const int nb = (n + TB - 1) / TB;
     int *flags = (int *)(aux + of), *epoch = flags + 2 * nb;
+    const int single = sizeof(R) == 4;
+    if (sb && nrhs <= 8 && m25_sb_enabled(n, single)) {
+        // 256-row diagonal blocks, the chain between blocks one product a block (trsv_sb.cu)
+        unsigned char *sbd = aux + sb_offset(n, single);
+        k_bump_epoch<<<1, 1, 0, s>>>(epoch);
+        M25_LAUNCH_CHECK("k_bump_epoch");
+        int rc = m25_sb_solve(A, lda, n, single, sbd, B, W1, nrhs, 0, epoch, err, s);   // U^T y = b
+        if (!rc) rc = m25_sb_solve(A, lda, n, single, sbd, W1, W2, nrhs, 1, epoch, err, s);   // L^T z = y
+        if (rc) return rc;
+        long tot = (long)n * nrhs;                                          // X = P z
+        k_gather_rows<R><<<(tot + 255) / 256, 256, 0, s>>>(W2, B, perm, n, nrhs);
+        M25_LAUNCH_CHECK("k_gather_rows");
+        return M25_OK;
+    }
     // CTAs of the persistent solves: one an SM (measured at N = 18,788, complex64, 8 columns: 3.4 ms with 148 CTAs,
     // 4.8 / 5.3 / 6.6 ms with 100 / 74 / 59, each owning more consecutive blocks)
     const int G = std::max(1, std::min(sm_count(), nb));
@@ -2137,9 +2175,10 @@ extern "C" int m25_getrs_prepare(const void *d_LU, long lda, int n, const int *d
                                  size_t aux_bytes, void *stream)
 {
     M25_REQUIRE(d_LU && d_ipiv && d_aux && n >= 1 && lda >= n, "m25_getrs_prepare: LU, ipiv, aux, n >= 1");
-    return single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes, S(stream))
+    return single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes,
+                                              S(stream), true)
                   : getrs_prepare_impl<double>((const double *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes,
-                                               S(stream));
+                                               S(stream), true);
 }
 
 extern "C" int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void *d_aux, void *d_B, int nrhs, void *stream)
@@ -2148,9 +2187,9 @@ extern "C" int m25_getrs_aux(const void *d_LU, long lda, int n, int single, void
     M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs_aux: 1 to 16 right-hand sides a call");
     int *err = m25_dev_err_word();
     return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, S(stream),
-                                          err)
+                                          err, true)
                   : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)d_aux, (double *)d_B, nrhs,
-                                           S(stream), err);
+                                           S(stream), err, true);
 }
 
 extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream)
@@ -2172,12 +2211,13 @@ extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, i
 int m25_getrs_on_scratch(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
                          size_t aux_bytes, int *d_err, void *d_B, int nrhs, cudaStream_t s)
 {
-    int rc = single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes, s)
+    int rc = single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux, aux_bytes,
+                                                s, false)
                     : getrs_prepare_impl<double>((const double *)d_LU, lda, n, d_ipiv, (unsigned char *)d_aux,
-                                                 aux_bytes, s);
+                                                 aux_bytes, s, false);
     if (rc) return rc;
     return single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)d_aux, (float *)d_B, nrhs, s,
-                                          d_err)
+                                          d_err, false)
                   : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)d_aux, (double *)d_B, nrhs,
-                                           s, d_err);
+                                           s, d_err, false);
 }

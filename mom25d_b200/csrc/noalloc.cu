@@ -6,7 +6,8 @@
 #include "common.cuh"
 
 // The scratch of m25_getrs_noalloc: the diagonal-block inverses, the permutation, two n x nrhs work vectors and
-// the solves' flags (the m25_getrs_aux_bytes layout). Its contents need not start at zero: every call zeroes the
+// the solves' flags (the layout of the 64-row-block solves, m25_getrs_aux_bytes_basic; this entry point
+// always solves that way). Its contents need not start at zero: every call zeroes the
 // flags it waits on before its solves read them.
 static __device__ __align__(256) unsigned char g_getrs_scratch[M25_GETRS_NOALLOC_MAX_BYTES];
 // The device status word of those solves (zero at module load; a bounded wait that gave up writes its code here).
@@ -14,6 +15,7 @@ static __device__ int g_getrs_status;
 
 int m25_getrs_on_scratch(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_aux,
                          size_t aux_bytes, int *d_err, void *d_B, int nrhs, cudaStream_t s);
+size_t m25_getrs_aux_bytes_basic(int n, int single);
 
 namespace {
 struct Scratch { void *aux = nullptr; int *status = nullptr; };
@@ -53,7 +55,7 @@ extern "C" int m25_getrs_noalloc(const void *d_LU, long lda, int n, const int *d
 {
     M25_REQUIRE(d_LU && d_ipiv && d_B && n >= 1 && lda >= n, "m25_getrs_noalloc: LU, ipiv, B, n >= 1");
     M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs_noalloc: 1 to 16 right-hand sides a call");
-    const size_t need = m25_getrs_aux_bytes(n, single);
+    const size_t need = m25_getrs_aux_bytes_basic(n, single);     // the 64-row-block solves' data
     if (need > (size_t)M25_GETRS_NOALLOC_MAX_BYTES) {
         char buf[200];
         snprintf(buf, sizeof buf, "m25_getrs_noalloc: n = %d (%s) needs %zu scratch bytes, above the fixed %zu "
