@@ -288,6 +288,7 @@ def run_gpu(args, rank, world):
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = e0.elapsed_time(e1) / 1000.0
+    solve_ms = time_solve_pair(ds, E_dev.shape[1])
     t_dev, t_e2e, t64 = max_over_ranks([t_dev, t_e2e, sum(lat64) / 1000.0], world, 'cuda')
     if rank != 0:
         return None
@@ -339,6 +340,8 @@ def run_gpu(args, rank, world):
                      "bound": "tensor", "achieved": round(achieved, 2), "peak": tensor_peak, "unit": "TFLOP/s",
                      "frac": round(achieved / tensor_peak, 4), "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else "fallback"},
+        "roofline_fill": fill_roofline(geo, phases.get('fill')),
+        "roofline_solve": solve_roofline(N, solve_ms, E_dev.shape[1], peaks.get('hbm_gbs')),
         "clocks": clocks,
     }
     if not args.no_cpu_baseline and world == 1:
@@ -354,6 +357,66 @@ def run_gpu(args, rank, world):
                                           f"fast.py:704-850, 996-1084) at full size, N={N}; seconds: " +
                                           ", ".join(f"{k} {v:.2f}" for k, v in cph.items())}
     return line
+
+
+def time_solve_pair(ds, k, reps=10):
+    """Device time (ms) of one complex64 solve pair (m25_getrs_aux: U^T then L^T, k right-hand sides) with the most
+    recently kept complex64 factor: the median of `reps` after 3 untimed, CUDA events on the solver's stream."""
+    import torch
+    from mom25d_b200 import _lib
+    if not ds.kept:
+        return None
+    rec = ds.kept[-1][1]
+    N = rec['Z'].shape[0]
+    L, st = _lib.lib(), ds.s
+    g = torch.Generator(device='cuda').manual_seed(3)
+    R = torch.complex(torch.randn(N, k, generator=g, device='cuda'), torch.randn(N, k, generator=g, device='cuda'))
+    X = R.clone()
+    stream = ds.stream if ds.stream is not None else torch.cuda.current_stream()
+    times = []
+    for i in range(3 + reps):
+        X.copy_(R)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _lib.check(L.m25_getrs_aux(_lib.P(rec['Z']), ctypes.c_long(N), ctypes.c_int(N), ctypes.c_int(1),
+                                   _lib.P(rec['aux']), _lib.P(X), ctypes.c_int(k), st), 'm25_getrs_aux')
+        b.record(stream)
+        b.synchronize()
+        if i >= 3:
+            times.append(a.elapsed_time(b))
+    _lib.sync_check(ds.stream)
+    return statistics.median(times)
+
+
+# FP64 flops of the fill per Z entry (edge tiles: 56 an entry + 30 a kernel evaluation, 0.95 evaluations an entry)
+FILL_FLOPS_PER_ENTRY = 56 + 30 * 0.95
+FP64_PEAK_TFLOPS = 36.6                  # a loop of independent FP64 FMAs over 148 x 8 CTAs of 256 threads, this B200
+
+
+def fill_roofline(geo, fill_ms):
+    """The fill's roofline (far fill + near correction, double precision, once a step): Ne^2 entries x 84.5 flops
+    against the FP64 FMA rate measured on this pool's B200 (no FP64 figure in MEASURED_PEAKS.json)."""
+    if not fill_ms:
+        return None
+    achieved = geo.Ne ** 2 * FILL_FLOPS_PER_ENTRY / (fill_ms / 1000.0) / 1e12
+    return {"kernel": "far fill + near correction in FP64 (m25_fill_far, m25_near), Ne^2 x 84.5 flops a fill",
+            "bound": "fp64", "achieved": round(achieved, 2), "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+            "frac": round(achieved / FP64_PEAK_TFLOPS, 4), "ms": fill_ms,
+            "peak_source": "FP64 FMA loop measured on this pool's B200 (not in MEASURED_PEAKS.json)"}
+
+
+def solve_roofline(N, ms, k, hbm):
+    """The complex64 solve pair's roofline: the factor's two triangles (8 N^2 bytes) plus, at N >= 2,048, the 256-row
+    blocks' inverses and couplings (2 x 3 x 256^2 complex64 entries a block), read once a pair, against HBM."""
+    if not ms or not hbm:
+        return None
+    ns = -(-N // 256)
+    nbytes = 8.0 * N * N + (6.0 * ns * 256 * 256 * 8 if N >= 2048 else 0.0)
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    return {"kernel": f"complex64 solve pair with {k} right-hand sides (m25_getrs_aux)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "ms_per_pair": round(ms, 3), "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
 
 
 def run_reference(args, rank, world):

@@ -578,15 +578,16 @@ static int sb_sms()
     return sms;
 }
 
-// Whether the solves of a factor of size n take this form: complex64, n >= SB_MIN_N, a CTA's chunks within
-// SB_CHMAX; M25_TRSV=pipe keeps the 64-row-block solves everywhere.
+// Whether the solves of a factor of size n take this form: n >= SB_MIN_N and a CTA's chunks within SB_CHMAX, for
+// complex64 and complex128 factors; M25_TRSV=pipe keeps the 64-row-block solves everywhere, M25_TRSV=c64 keeps them
+// for complex128 factors.
 bool m25_sb_enabled(int n, int single)
 {
     static const int on = [] {
         const char *e = getenv("M25_TRSV");
-        return (e && !strcmp(e, "pipe")) ? 0 : 1;
+        return (e && !strcmp(e, "pipe")) ? 0 : (e && !strcmp(e, "c64")) ? 1 : 2;
     }();
-    if (!on || !single || n < SB_MIN_N) return false;
+    if (!on || (!single && on < 2) || n < SB_MIN_N) return false;
     const int GB = sb_sms() - SB_GA, nch = (n + SBC - 1) / SBC;
     return GB > 0 && (nch + GB - 1) / GB <= SB_CHMAX;
 }

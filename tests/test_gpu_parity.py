@@ -345,44 +345,47 @@ def test_complex64_solves_over_several_blocks_a_cta(n, nrhs):
         assert err < 1e-4, err
 
 
-@pytest.mark.parametrize('n,nrhs', [(2048, 8), (2049, 1), (2301, 5), (5000, 8), (18788, 8)])
-def test_complex64_solves_by_256_row_blocks(n, nrhs):
-    """The complex64 solves by 256-row diagonal blocks (inverted once per factor, with their couplings to the two
-    blocks solved before them: one product a block along the chain): whole and ragged last blocks and chunks
-    (2048, 2049: a last block of one row), odd n (8-byte copies of the factor tiles), 1 to 8 right-hand sides, a
-    factor whose every column takes a row interchange; against the complex128 solve of the same Z, twice in a row
-    (the flags' epochs)."""
+@pytest.mark.parametrize('n,nrhs,single', [(2048, 8, 1), (2049, 1, 1), (2301, 5, 1), (5000, 8, 1), (18788, 8, 1),
+                                           (2049, 3, 0), (5000, 8, 0)])
+def test_solves_by_256_row_blocks(n, nrhs, single):
+    """The solves by 256-row diagonal blocks (inverted once per factor, with their couplings to the two blocks
+    solved before them: one product a block along the chain), complex64 and complex128: whole and ragged last blocks
+    and chunks (2048, 2049: a last block of one row), odd n (8-byte copies of complex64 factor tiles), 1 to 8
+    right-hand sides, a factor whose every column takes a row interchange; against the complex128 solve of the same
+    Z, twice in a row (the flags' epochs)."""
     from mom25d_b200 import _lib
     L = _lib.lib()
     L.m25_getrs_aux_bytes.restype = ctypes.c_size_t
+    rdt, cdt = (torch.float32, torch.complex64) if single else (torch.float64, torch.complex128)
     g = torch.Generator(device='cuda').manual_seed(n)
     sigma = torch.randperm(n, generator=g, device='cuda')
-    A = 0.1 * torch.complex(torch.randn(n, n, generator=g, device='cuda'), torch.randn(n, n, generator=g, device='cuda'))
-    phase = 2 * np.pi * torch.rand(n, generator=g, device='cuda')
-    A[sigma, torch.arange(n, device='cuda')] += 10 * n * torch.exp(1j * phase).to(torch.complex64)
+    A = 0.1 * torch.complex(torch.randn(n, n, generator=g, device='cuda', dtype=rdt),
+                            torch.randn(n, n, generator=g, device='cuda', dtype=rdt))
+    phase = 2 * np.pi * torch.rand(n, generator=g, device='cuda', dtype=rdt)
+    A[sigma, torch.arange(n, device='cuda')] += 10 * n * torch.exp(1j * phase).to(cdt)
     Z = A.T.contiguous()
-    R = torch.complex(torch.randn(n, nrhs, generator=g, device='cuda'), torch.randn(n, nrhs, generator=g,
-                                                                                     device='cuda'))
+    R = torch.complex(torch.randn(n, nrhs, generator=g, device='cuda', dtype=rdt),
+                      torch.randn(n, nrhs, generator=g, device='cuda', dtype=rdt))
     x = torch.linalg.solve(Z.to(torch.complex128), R.to(torch.complex128))
     F = Z.clone()
     ipiv = torch.empty(n, dtype=torch.int32, device='cuda')
-    nb = int(L.m25_getrf_workspace(n, 1))
+    nb = int(L.m25_getrf_workspace(n, single))
     work = torch.empty(nb, dtype=torch.uint8, device='cuda')
-    _lib.check(L.m25_getrf(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 1, 1, _lib.P(work), ctypes.c_size_t(nb),
-                           _lib.stream_ptr()))
+    _lib.check(L.m25_getrf(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), single, single, _lib.P(work),
+                           ctypes.c_size_t(nb), _lib.stream_ptr()))
     del work
     assert (ipiv.cpu().numpy() != np.arange(n)).mean() > 0.9
-    na = int(L.m25_getrs_aux_bytes(n, 1))
+    na = int(L.m25_getrs_aux_bytes(n, single))
     aux = torch.empty(na, dtype=torch.uint8, device='cuda')
-    _lib.check(L.m25_getrs_prepare(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), 1, _lib.P(aux), ctypes.c_size_t(na),
-                                   _lib.stream_ptr()), 'm25_getrs_prepare')
+    _lib.check(L.m25_getrs_prepare(_lib.P(F), ctypes.c_long(n), n, _lib.P(ipiv), single, _lib.P(aux),
+                                   ctypes.c_size_t(na), _lib.stream_ptr()), 'm25_getrs_prepare')
     for _ in range(2):
         X = R.clone()
-        _lib.check(L.m25_getrs_aux(_lib.P(F), ctypes.c_long(n), n, 1, _lib.P(aux), _lib.P(X), nrhs,
+        _lib.check(L.m25_getrs_aux(_lib.P(F), ctypes.c_long(n), n, single, _lib.P(aux), _lib.P(X), nrhs,
                                    _lib.stream_ptr()), 'm25_getrs_aux')
         _lib.sync_check()
         err = (X.to(torch.complex128) - x).abs().max().item() / x.abs().max().item()
-        assert err < 1e-5, err
+        assert err < (1e-5 if single else 1e-12), err
 
 
 @pytest.mark.parametrize('n,nrhs', [(9509, 1), (18788, 8), (19000, 16)])
