@@ -338,9 +338,11 @@ __device__ __forceinline__ bool sb_wait_flags(const int *flags, int c0, int cnt,
     return *ok != 0;
 }
 
-template <typename R, int NBUF>
+// NBUF: tiles in the ring; TPB: tiles a product waits for at once (1, or a whole task of 4 with NBUF = 8)
+template <typename R, int NBUF, int TPB>
 __global__ void __launch_bounds__(SB_NT, 1) k_trsv_sb(SbSolve<R> a)
 {
+    static_assert(SB_KTS % TPB == 0 && NBUF >= 2 * TPB, "whole batches, one in flight beside the one in use");
     typedef cpx<R> C;
     constexpr int XS = sb_xs<R>();
     extern __shared__ __align__(16) unsigned char sb_raw[];
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(SB_NT, 1) k_trsv_sb(SbSolve<R> a)
             slots[e] = (row < n && cc < nrhs) ? a.Tin[(size_t)row * nrhs + cc] : mk<R>(0, 0);
         }
     if (tid == 0) ok = 1;
-    for (int i = 0; i < NBUF - 1; ++i) issue();
+    for (int i = 0; i < NBUF - TPB; ++i) issue();
     __syncthreads();
     // one staged vector of SB rows: from src (row stride ld, columns < cols), rows past n and columns past cols zero;
     // every load before any store
@@ -548,13 +550,17 @@ __global__ void __launch_bounds__(SB_NT, 1) k_trsv_sb(SbSolve<R> a)
         C acc[SB_NR];
 #pragma unroll
         for (int j = 0; j < SB_NR; ++j) acc[j] = mk<R>(0, 0);
-        for (int kt = 0; kt < SB_KTS; ++kt) {
-            issue();
-            sb_wait_group<NBUF - 1>();                                // this tile's copies have landed
+        for (int kt0 = 0; kt0 < SB_KTS; kt0 += TPB) {
+#pragma unroll
+            for (int i = 0; i < TPB; ++i) issue();
+            sb_wait_group<NBUF - TPB>();                              // this batch's copies have landed
             __syncthreads();
-            sb_acc_tile<R>(tiles + (size_t)(used % NBUF) * SBC * SB_TS, Xs + (size_t)kt * SB_KT * XS, acc);
-            ++used;
-            __syncthreads();                                          // (the buffer is the next copy's)
+#pragma unroll
+            for (int i = 0; i < TPB; ++i) {
+                sb_acc_tile<R>(tiles + (size_t)(used % NBUF) * SBC * SB_TS, Xs + (size_t)(kt0 + i) * SB_KT * XS, acc);
+                ++used;
+            }
+            __syncthreads();                                          // (the buffers are the next copies')
         }
         const C v = sb_reduce_scatter<R>(acc);
         if (!(tid & 1)) {                                             // lanes h, h ^ 1 hold column h / 2
@@ -660,18 +666,24 @@ static int sb_solve_impl(const cpx<R> *A, long lda, int n, unsigned char *sb, co
                     Tin, Xout, reinterpret_cast<cpx<R> *>(sb + otx), nrhs, backward,
                     (int)((lda % 2 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0)),
                     flags + (size_t)tri * 2 * nch, flags + (size_t)tri * 2 * nch + nch, epoch, err};
-    // the tile ring's depth: 5 tiles (3, 5 and 8 measured the same at N = 18,788: the ring is not what binds);
-    // M25_SB_NBUF=3|5|8 overrides
+    // the tile ring: complex64, 8 tiles whose products wait for a task's 4 tiles at once (two barriers a task instead
+    // of eight: 1.94 against 2.07 ms a pair at N = 18,788); M25_SB_TPB=1 waits for one tile at a time in a ring of
+    // M25_SB_NBUF=3|5|8 (default 5; the depth alone measured the same). complex128 takes 3 single tiles, its tiles
+    // being twice as large
     static const int want = [] { const char *e = getenv("M25_SB_NBUF"); return e ? atoi(e) : 5; }();
+    static const int tpb = [] { const char *e = getenv("M25_SB_TPB"); return e ? atoi(e) : 4; }();
     int optin = 0, dev = 0;
     M25_CHECK(cudaGetDevice(&dev));
     M25_CHECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     int nbuf = want >= 8 ? 8 : want >= 5 ? 5 : 3;
+    const bool batch4 = sizeof(R) == 4 && tpb == 4 && sb_smem<R>(8) <= (size_t)optin;
+    if (batch4) nbuf = 8;
     while (nbuf > 3 && sb_smem<R>(nbuf) > (size_t)optin) nbuf = nbuf == 8 ? 5 : 3;
     const size_t sm = sb_smem<R>(nbuf);
     M25_REQUIRE(sm <= (size_t)optin, "m25_sb_solve: shared memory");
-    const void *kf = nbuf == 8 ? (const void *)k_trsv_sb<R, 8> : nbuf == 5 ? (const void *)k_trsv_sb<R, 5>
-                                                                           : (const void *)k_trsv_sb<R, 3>;
+    const void *kf = batch4 ? (const void *)k_trsv_sb<R, 8, 4>
+                   : nbuf == 8 ? (const void *)k_trsv_sb<R, 8, 1> : nbuf == 5 ? (const void *)k_trsv_sb<R, 5, 1>
+                                                                         : (const void *)k_trsv_sb<R, 3, 1>;
     M25_CHECK(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     void *kargs[] = {&args};
     M25_CHECK(cudaLaunchCooperativeKernel(kf, dim3(G), dim3(SB_NT), kargs, sm, s));
