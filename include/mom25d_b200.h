@@ -257,7 +257,8 @@ int m25_getrf(void *d_A, long lda, int n, int *d_ipiv, int single, int tf32, voi
 int m25_set_lu_tuning(int single, const int *h_n, const int *h_nb2, const int *h_blocks, int count);
 int m25_get_lu_tuning(int n, int single, int *nb2, int *blocks);
 /* Solves Z X = B with the factor of Z^T (lu_solve(..., trans=1)); B (row-major n x nrhs, complex in the factor's
- * precision) overwritten by X. */
+ * precision) overwritten by X. One call: its scratch from the stream-ordered allocator, by 64-row diagonal blocks
+ * (for many solves with one factor, m25_getrs_prepare / m25_getrs_aux below). */
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);
 /* The solves split for a factor that is solved with many times (the refinement's preconditioner, the backend's
  * solve(R)): m25_getrs_prepare inverts the factor's diagonal blocks once into d_aux (m25_getrs_aux_bytes) and

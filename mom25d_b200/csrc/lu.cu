@@ -2196,11 +2196,21 @@ extern "C" int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, i
 {
     M25_REQUIRE(d_LU && d_ipiv && d_B && n >= 1 && lda >= n, "m25_getrs: LU, ipiv, B, n >= 1");
     M25_REQUIRE(nrhs >= 1 && nrhs <= 16, "m25_getrs: 1 to 16 right-hand sides a call");
-    const size_t bytes = m25_getrs_aux_bytes(n, single);
+    // one call: by 64-row diagonal blocks (the 256-row blocks' inverses and couplings pay off only over many solves
+    // with one factor, m25_getrs_prepare / m25_getrs_aux)
+    const size_t bytes = m25_getrs_aux_bytes_basic(n, single);
     void *aux = nullptr;
     M25_CHECK(cudaMallocAsync(&aux, bytes, S(stream)));
-    int rc = m25_getrs_prepare(d_LU, lda, n, d_ipiv, single, aux, bytes, stream);
-    if (!rc) rc = m25_getrs_aux(d_LU, lda, n, single, aux, d_B, nrhs, stream);
+    int *err = m25_dev_err_word();
+    int rc = single ? getrs_prepare_impl<float>((const float *)d_LU, lda, n, d_ipiv, (unsigned char *)aux, bytes,
+                                                S(stream), false)
+                    : getrs_prepare_impl<double>((const double *)d_LU, lda, n, d_ipiv, (unsigned char *)aux, bytes,
+                                                 S(stream), false);
+    if (!rc)
+        rc = single ? getrs_aux_impl<float>((const float *)d_LU, lda, n, (unsigned char *)aux, (float *)d_B, nrhs,
+                                            S(stream), err, false)
+                    : getrs_aux_impl<double>((const double *)d_LU, lda, n, (unsigned char *)aux, (double *)d_B, nrhs,
+                                             S(stream), err, false);
     cudaError_t fe = cudaFreeAsync(aux, S(stream));
     if (!rc && fe != cudaSuccess) return m25_cuda_status(fe, "cudaFreeAsync");
     return rc;
