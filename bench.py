@@ -17,6 +17,7 @@ default path at this size (mixed precision, kept complex64 LUs), at full size.
 """
 import argparse
 import ctypes
+import gc
 import json
 import os
 import statistics
@@ -234,6 +235,8 @@ def run_gpu(args, rank, world):
     cold()
     lat, lu_ms, iters, paths, kept_X, step_path = [], [], [], {}, [], []
     ds.timings, ds.attempts = {}, []
+    gc.collect()
+    gc.disable()                            # no collector pause inside a timed region (as timeit does)
     ev0.record(stream)
     for i in range(args.steps):
         ph0 = dict(ds.timings) if args.verbose else None
@@ -252,6 +255,7 @@ def run_gpu(args, rank, world):
                   "  residual by step: " + ' '.join(f"{x:.0e}" for x in rh[1::3]), file=sys.stderr)
     ev1.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     clocks = clk.stop()
     launches = lib.m25_launch_count() - n0
     t_dev = ev0.elapsed_time(ev1) / 1000.0
@@ -282,11 +286,14 @@ def run_gpu(args, rank, world):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cold()
+    gc.collect()
+    gc.disable()
     e0.record(stream)
     for i in range(args.steps):
         sim.sparams(mine[i % len(mine)])
     e1.record(stream)
     torch.cuda.synchronize()
+    gc.enable()
     t_e2e = e0.elapsed_time(e1) / 1000.0
     solve_ms = time_solve_pair(ds, E_dev.shape[1])
     t_dev, t_e2e, t64 = max_over_ranks([t_dev, t_e2e, sum(lat64) / 1000.0], world, 'cuda')
@@ -343,6 +350,7 @@ def run_gpu(args, rank, world):
         "roofline_fill": fill_roofline(geo, phases.get('fill')),
         "roofline_solve": solve_roofline(N, solve_ms, E_dev.shape[1], peaks.get('hbm_gbs')),
         "clocks": clocks,
+        "host": "Python's garbage collector off inside the timed regions (collected before each)",
     }
     if not args.no_cpu_baseline and world == 1:
         from oracle import solve as osolve
