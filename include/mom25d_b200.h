@@ -262,7 +262,8 @@ int m25_get_lu_tuning(int n, int single, int *nb2, int *blocks);
 int m25_getrs(const void *d_LU, long lda, int n, const int *d_ipiv, int single, void *d_B, int nrhs, void *stream);
 /* The solves split for a factor that is solved with many times (the refinement's preconditioner, the backend's
  * solve(R)): m25_getrs_prepare inverts the factor's diagonal blocks once into d_aux (m25_getrs_aux_bytes) and
- * keeps the pivots there; m25_getrs_aux then solves like m25_getrs from d_aux. d_aux belongs to one factor. For a
+ * keeps the pivots there; m25_getrs_aux then solves like m25_getrs from d_aux. d_aux belongs to one factor, and its
+ * solves run one at a time (they share its flags and work vectors: two on different streams race). For a
  * factor of n >= 2048, d_aux also holds the inverses of its 256-row diagonal blocks and their couplings with the
  * two blocks before them (three 256 x 256 matrices a block a triangle), with which solves of up to 8 right-hand
  * sides take one product a block along their chain (M25_TRSV=pipe: not; M25_TRSV=c64: complex64 factors only). */
